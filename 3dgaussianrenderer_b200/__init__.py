@@ -1,0 +1,419 @@
+"""gs_b200: B200-native 3D Gaussian splatting frame pipeline.
+
+Python binding of the C ABI in include/gs_b200.h (libgs_b200.so, built
+in-tree for sm_100a by ``make -C 3dgaussianrenderer_b200/csrc``).  The
+binding is thin: device memory comes from PyTorch tensors (or raw
+pointers), every call goes straight to the CUDA library, and there is no
+CPU fallback -- importing this module fails loudly when the library is
+missing.
+
+The package name starts with a digit, so import it with
+``importlib.import_module("3dgaussianrenderer_b200")``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass, field
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgs_b200.so")
+HEADER_PATH = os.path.join(os.path.dirname(_HERE), "include", "gs_b200.h")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"{LIB_PATH} is missing: build it with `make -C {os.path.join(_HERE, 'csrc')}` "
+        "(there is no CPU fallback)")
+
+lib = ctypes.CDLL(LIB_PATH)
+
+GS_OK = 0
+GS_ERR_INVALID = 1
+GS_ERR_OOM = 2
+GS_ERR_CAPACITY = 3
+GS_ERR_DEVICE_TIMEOUT = 4
+GS_ERR_CUDA = 5
+GS_ERR_NO_DEVICE = 6
+GS_TERM_REFERENCE = 0
+GS_TERM_TMIN = 1
+
+
+class GsError(RuntimeError):
+    def __init__(self, status: int, where: str):
+        self.status = status
+        msg = lib.gs_status_string(status).decode()
+        detail = lib.gs_last_error_string().decode()
+        super().__init__(f"{where}: {msg} ({detail})")
+
+
+class gs_camera(ctypes.Structure):
+    _fields_ = [
+        ("view", ctypes.c_float * 16),
+        ("position", ctypes.c_float * 3),
+        ("fov_cotangent", ctypes.c_float * 2),
+        ("depth_scale_bias", ctypes.c_float * 2),
+        ("aspect", ctypes.c_float),
+        ("width", ctypes.c_int32),
+        ("height", ctypes.c_int32),
+    ]
+
+
+class gs_render_cfg(ctypes.Structure):
+    _fields_ = [
+        ("sh_max_degree", ctypes.c_int32),
+        ("termination", ctypes.c_int32),
+        ("t_min", ctypes.c_float),
+        ("tile_w", ctypes.c_int32),
+        ("tile_h", ctypes.c_int32),
+        ("raster_batch", ctypes.c_int32),
+    ]
+
+
+class gs_stats(ctypes.Structure):
+    _fields_ = [
+        ("sh_eval_ms", ctypes.c_double),
+        ("project_ms", ctypes.c_double),
+        ("build_tile_ms", ctypes.c_double),
+        ("sort_ms", ctypes.c_double),
+        ("raster_ms", ctypes.c_double),
+        ("total_ms", ctypes.c_double),
+        ("num_keys", ctypes.c_int64),
+        ("num_tiles", ctypes.c_int64),
+        ("kernel_launches", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_P = ctypes.c_void_p
+_I = ctypes.c_int
+_I32 = ctypes.c_int32
+_I64 = ctypes.c_int64
+_F = ctypes.c_float
+
+
+def _sig(name, restype, *argtypes):
+    fn = getattr(lib, name)
+    fn.restype = restype
+    fn.argtypes = list(argtypes)
+    return fn
+
+
+_sig("gs_version", _I)
+_sig("gs_status_string", ctypes.c_char_p, _I)
+_sig("gs_last_error_string", ctypes.c_char_p)
+_sig("gs_default_cfg", None, ctypes.POINTER(gs_render_cfg))
+_sig("gs_camera_look_at", None, ctypes.POINTER(gs_camera), ctypes.POINTER(_F), ctypes.POINTER(_F),
+     ctypes.POINTER(_F), _F, _I32, _I32, _F, _F)
+_sig("gs_ctx_create", _I, _I, ctypes.POINTER(_P))
+_sig("gs_ctx_destroy", _I, _P)
+_sig("gs_ctx_device_bytes", _I64, _P)
+_sig("gs_scene_create", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.POINTER(_P))
+_sig("gs_scene_destroy", _I, _P)
+_sig("gs_scene_size", _I64, _P)
+_sig("gs_scene_device_bytes", _I64, _P)
+_sig("gs_render", _I, _P, _P, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P,
+     ctypes.POINTER(gs_stats), _P)
+_sig("gs_render_host", _I, _P, _P, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P,
+     ctypes.POINTER(gs_stats), _P)
+_sig("gs_render_batch", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(gs_render_cfg),
+     ctypes.POINTER(_P), ctypes.POINTER(gs_stats), _P)
+_sig("gs_render_batch_host", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(gs_render_cfg), _P,
+     ctypes.POINTER(gs_stats), _P)
+_sig("gs_stage_sh", _I, _I64, _P, _P, _I32, _I32, ctypes.POINTER(gs_camera), _P, _P)
+_sig("gs_stage_project", _I, _I64, _P, _P, ctypes.POINTER(gs_camera), _P, _P, _P, _P, _P)
+_sig("gs_stage_build", _I, _P, _I64, _P, _P, _P, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P, _P,
+     _I64, ctypes.POINTER(_I64), _P)
+_sig("gs_stage_sort", _I, _P, _I64, _I32, _P, _P, _P, _P, ctypes.POINTER(_I32), _P)
+_sig("gs_stage_ranges", _I, _I64, _P, _I64, _P, _P)
+_sig("gs_stage_raster", _I, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P, _P, _P, _P, _P, _P, _P)
+_sig("gs_num_tiles", _I64, _I32, _I32, ctypes.POINTER(gs_render_cfg))
+_sig("gs_key_bits", _I32, _I64)
+
+
+def check(status: int, where: str) -> None:
+    if status != GS_OK:
+        raise GsError(status, where)
+
+
+def _ptr(x) -> int | None:
+    """Device/host address of a torch tensor, numpy array or int."""
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    if isinstance(x, np.ndarray):
+        return x.ctypes.data
+    return x.data_ptr()
+
+
+def _stream_ptr(stream) -> int | None:
+    if stream is None:
+        return None
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+# ---------------------------------------------------------------------------
+# Camera (core/camera.h:11-59) and render options
+# ---------------------------------------------------------------------------
+
+class Camera:
+    """Pinhole camera with the reference Camera's setters and getters
+    (core/camera.h:11-59).  Depth uses the built frame loop's convention
+    (app/main.cpp:352-358): clip z = -2/(f-n) * z_view - (f+n)/(f-n)."""
+
+    def __init__(self):
+        self._fovy = np.radians(50.0)
+        self._w, self._h = 1024, 1024
+        self._near, self._far = 0.01, 100.0
+        self._eye = np.array([0.0, 0.0, 3.0], np.float32)
+        self._target = np.zeros(3, np.float32)
+        self._up = np.array([0.0, 1.0, 0.0], np.float32)
+        self._update()
+
+    def SetFovY(self, fov_y_rad: float):
+        self._fovy = float(fov_y_rad)
+        self._update()
+
+    def SetResolution(self, width: int, height: int):
+        self._w, self._h = int(width), int(height)
+        self._update()
+
+    def SetNearFar(self, near: float, far: float):
+        self._near, self._far = float(near), float(far)
+        self._update()
+
+    def SetPose(self, position, look_at, up=(0.0, 1.0, 0.0)):
+        self._eye = np.asarray(position, np.float32)
+        self._target = np.asarray(look_at, np.float32)
+        self._up = np.asarray(up, np.float32)
+        self._update()
+
+    def _update(self):
+        c = gs_camera()
+        eye = (_F * 3)(*self._eye.tolist())
+        tgt = (_F * 3)(*self._target.tolist())
+        up = (_F * 3)(*self._up.tolist())
+        lib.gs_camera_look_at(ctypes.byref(c), eye, tgt, up, _F(self._fovy), self._w, self._h, _F(self._near),
+                              _F(self._far))
+        self.c = c
+
+    def GetView(self):
+        return np.array(self.c.view, np.float32).reshape(4, 4)  # [col][row]
+
+    def GetPosition(self):
+        return np.array(self.c.position, np.float32)
+
+    def GetAspect(self):
+        return float(self.c.aspect)
+
+    def GetFovCotangent(self):
+        return np.array(self.c.fov_cotangent, np.float32)
+
+    def GetDepthScaleBias(self):
+        return np.array(self.c.depth_scale_bias, np.float32)
+
+    def GetWidth(self):
+        return self._w
+
+    def GetHeight(self):
+        return self._h
+
+    def GetFovY(self):
+        return self._fovy
+
+    def GetZNear(self):
+        return self._near
+
+    def GetZFar(self):
+        return self._far
+
+
+def look_at(eye, target, up=(0.0, 1.0, 0.0), fovy_deg=50.0, width=1024, height=1024, near=0.1, far=100.0) -> Camera:
+    cam = Camera()
+    cam._fovy = float(np.radians(fovy_deg))
+    cam._w, cam._h = int(width), int(height)
+    cam._near, cam._far = float(near), float(far)
+    cam._eye = np.asarray(eye, np.float32)
+    cam._target = np.asarray(target, np.float32)
+    cam._up = np.asarray(up, np.float32)
+    cam._update()
+    return cam
+
+
+@dataclass
+class RenderConfig:
+    """Pipeline options (gs_render_cfg).  reference() gives the reference
+    renderer's behaviour (SH degree <= 2, tile-wide T <= 0.02 termination
+    at 32-entry granularity); the default is full SH-3 with per-pixel
+    T < 1e-4 termination."""
+    sh_max_degree: int = 3
+    termination: int = GS_TERM_TMIN
+    t_min: float = 1e-4
+    tile_w: int = 16
+    tile_h: int = 16
+    raster_batch: int = 0
+
+    @staticmethod
+    def reference() -> "RenderConfig":
+        return RenderConfig(sh_max_degree=2, termination=GS_TERM_REFERENCE, t_min=1e-4, tile_w=16, tile_h=16)
+
+    def c(self) -> gs_render_cfg:
+        return gs_render_cfg(self.sh_max_degree, self.termination, self.t_min, self.tile_w, self.tile_h,
+                             self.raster_batch)
+
+
+def num_tiles(width: int, height: int, cfg: RenderConfig) -> int:
+    c = cfg.c()
+    return int(lib.gs_num_tiles(width, height, ctypes.byref(c)))
+
+
+def key_bits(tiles: int) -> int:
+    return int(lib.gs_key_bits(tiles))
+
+
+# ---------------------------------------------------------------------------
+# Context / scene / frame
+# ---------------------------------------------------------------------------
+
+class Context:
+    def __init__(self, device: int = 0):
+        h = _P()
+        check(lib.gs_ctx_create(device, ctypes.byref(h)), "gs_ctx_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.gs_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def device_bytes(self) -> int:
+        return int(lib.gs_ctx_device_bytes(self.h))
+
+
+class Scene:
+    """Device-resident scene (Renderer::UploadModel)."""
+
+    def __init__(self, ctx: Context, pos4: np.ndarray, sr4: np.ndarray, sh_grouped: np.ndarray | None,
+                 sh_degree: int, color4: np.ndarray | None = None):
+        self.ctx = ctx
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        sr4 = np.ascontiguousarray(sr4, np.float32)
+        n = pos4.shape[0]
+        col = None if color4 is None else np.ascontiguousarray(color4, np.float32)
+        sh = None if sh_grouped is None else np.ascontiguousarray(sh_grouped, np.float32)
+        h = _P()
+        check(lib.gs_scene_create(ctx.h, n, _ptr(pos4), _ptr(sr4), _ptr(col), _ptr(sh), sh_degree,
+                                  ctypes.byref(h)), "gs_scene_create")
+        self.h = h
+        self.n = n
+        self.sh_degree = sh_degree
+
+    def close(self):
+        if self.h:
+            lib.gs_scene_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def render(ctx: Context, scene: Scene, cam: Camera, cfg: RenderConfig, out_rgba, stream=None) -> dict:
+    """Renders into a device tensor (uint8, H*W*4)."""
+    st = gs_stats()
+    c = cfg.c()
+    check(lib.gs_render(ctx.h, scene.h, ctypes.byref(cam.c), ctypes.byref(c), _ptr(out_rgba), ctypes.byref(st),
+                        _stream_ptr(stream)), "gs_render")
+    return st.as_dict()
+
+
+def render_host(ctx: Context, scene: Scene, cam: Camera, cfg: RenderConfig, out: np.ndarray | None = None,
+                stream=None):
+    """Renders into host memory; returns (image HxWx4 uint8, stats)."""
+    if out is None:
+        out = np.zeros((cam.GetHeight(), cam.GetWidth(), 4), np.uint8)
+    st = gs_stats()
+    c = cfg.c()
+    check(lib.gs_render_host(ctx.h, scene.h, ctypes.byref(cam.c), ctypes.byref(c), _ptr(out), ctypes.byref(st),
+                             _stream_ptr(stream)), "gs_render_host")
+    return out, st.as_dict()
+
+
+def render_batch(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig, outs: list, stream=None) -> dict:
+    arr = (gs_camera * len(cams))(*[c.c for c in cams])
+    ptrs = (_P * len(outs))(*[_ptr(o) for o in outs])
+    st = gs_stats()
+    c = cfg.c()
+    check(lib.gs_render_batch(ctx.h, scene.h, arr, len(cams), ctypes.byref(c), ptrs, ctypes.byref(st),
+                              _stream_ptr(stream)), "gs_render_batch")
+    return st.as_dict()
+
+
+def render_batch_host(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig, out: np.ndarray,
+                      stream=None) -> dict:
+    arr = (gs_camera * len(cams))(*[c.c for c in cams])
+    st = gs_stats()
+    c = cfg.c()
+    check(lib.gs_render_batch_host(ctx.h, scene.h, arr, len(cams), ctypes.byref(c), _ptr(out), ctypes.byref(st),
+                                   _stream_ptr(stream)), "gs_render_batch_host")
+    return st.as_dict()
+
+
+# ---------------------------------------------------------------------------
+# Stage API (core/gaussian_render.cuh:113-126 equivalents)
+# ---------------------------------------------------------------------------
+
+def stage_sh(n, d_pos, d_sh, sh_count, eval_degree, cam: Camera, d_color, stream=None):
+    check(lib.gs_stage_sh(n, _ptr(d_pos), _ptr(d_sh), sh_count, eval_degree, ctypes.byref(cam.c), _ptr(d_color),
+                          _stream_ptr(stream)), "gs_stage_sh")
+
+
+def stage_project(n, d_pos, d_sr, cam: Camera, d_xy, d_z, d_ell, d_conic, stream=None):
+    check(lib.gs_stage_project(n, _ptr(d_pos), _ptr(d_sr), ctypes.byref(cam.c), _ptr(d_xy), _ptr(d_z), _ptr(d_ell),
+                               _ptr(d_conic), _stream_ptr(stream)), "gs_stage_project")
+
+
+def stage_build(ctx: Context, n, d_xy, d_z, d_ell, cam: Camera, cfg: RenderConfig, d_keys, d_values, capacity,
+                stream=None) -> int:
+    k = _I64(0)
+    c = cfg.c()
+    status = lib.gs_stage_build(ctx.h, n, _ptr(d_xy), _ptr(d_z), _ptr(d_ell), ctypes.byref(cam.c), ctypes.byref(c),
+                                _ptr(d_keys), _ptr(d_values), capacity, ctypes.byref(k), _stream_ptr(stream))
+    if status == GS_ERR_CAPACITY:
+        raise GsError(status, f"gs_stage_build (K={k.value})")
+    check(status, "gs_stage_build")
+    return int(k.value)
+
+
+def stage_sort(ctx: Context, num_keys, bits, d_keys, d_values, d_keys_alt, d_values_alt, stream=None) -> int:
+    sel = _I32(0)
+    check(lib.gs_stage_sort(ctx.h, num_keys, bits, _ptr(d_keys), _ptr(d_values), _ptr(d_keys_alt),
+                            _ptr(d_values_alt), ctypes.byref(sel), _stream_ptr(stream)), "gs_stage_sort")
+    return int(sel.value)
+
+
+def stage_ranges(num_keys, d_keys, tiles, d_ranges, stream=None):
+    check(lib.gs_stage_ranges(num_keys, _ptr(d_keys), tiles, _ptr(d_ranges), _stream_ptr(stream)), "gs_stage_ranges")
+
+
+def stage_raster(cam: Camera, cfg: RenderConfig, d_ranges, d_values, d_xy, d_conic, d_color, d_rgba, stream=None):
+    c = cfg.c()
+    check(lib.gs_stage_raster(ctypes.byref(cam.c), ctypes.byref(c), _ptr(d_ranges), _ptr(d_values), _ptr(d_xy),
+                              _ptr(d_conic), _ptr(d_color), _ptr(d_rgba), _stream_ptr(stream)), "gs_stage_raster")
+
+
+from . import scenes  # noqa: E402,F401

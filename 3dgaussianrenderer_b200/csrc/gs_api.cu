@@ -1,0 +1,808 @@
+// C-ABI of gs_b200: contexts, resident scenes, whole-frame and stage entry
+// points (declared in include/gs_b200.h).
+//
+// Frame orchestration replaces the reference's frame loop
+// (app/main.cpp:326-432) and Renderer::Render (core/renderer.cpp:94-139):
+// everything runs on one stream with events between stages; the only host
+// synchronisation inside a frame is the read of the exact key count K after
+// the fused projection/count kernel (the reference syncs after every stage
+// and once more for its tile counter).  Buffers grow on demand and are
+// never truncated: the tile list is sized from the exact K.
+#include "gs_kernels.h"
+#include "../../include/gs_b200.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace gs;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const char* what)
+{
+    g_last_error = what ? what : "";
+    return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where)
+{
+    g_last_error = std::string(where) + ": " + cudaGetErrorString(e);
+    if (e == cudaErrorMemoryAllocation) return GS_ERR_OOM;
+    if (e == cudaErrorNoKernelImageForDevice || e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return GS_ERR_NO_DEVICE;
+    return GS_ERR_CUDA;
+}
+
+#define GS_CUDA(call)                                            \
+    do {                                                         \
+        cudaError_t _e = (call);                                 \
+        if (_e != cudaSuccess) return cuda_fail(_e, #call);      \
+    } while (0)
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    // Grows to at least `need` bytes (25% headroom); old contents are lost.
+    cudaError_t ensure(size_t need, bool zero = false)
+    {
+        if (need <= bytes && p) return cudaSuccess;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        const size_t sz = std::max<size_t>(need + need / 4, 256);
+        cudaError_t e = cudaMalloc(&p, sz);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            return e;
+        }
+        bytes = sz;
+        if (zero) return cudaMemset(p, 0, sz);
+        return cudaSuccess;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const
+    {
+        return reinterpret_cast<T*>(p);
+    }
+};
+
+// Small per-context device words, cleared with one memset per frame.
+struct Counters {
+    unsigned long long frame_tile;                 // frame kernel block queue
+    unsigned long long raster_tile;                // persistent raster queue
+    unsigned long long sort_tiles[kMaxPasses];     // onesweep tile queues
+    int64_t total;                                 // K
+    int err;
+    int pad;
+};
+
+}  // namespace
+
+struct gs_scene {
+    int device = 0;
+    int64_t n = 0;
+    int32_t sh_degree = 0;
+    int32_t sh_count = 0;
+    DevBuf pos, sr, color, sh;
+};
+
+struct gs_ctx {
+    int device = 0;
+    int num_sms = 148;
+    std::mutex mu;
+    uint32_t epoch_scan = 1, epoch_sort = 1;
+    DevBuf views;                          // ViewParams[]
+    DevBuf color, xy, z, ell, conic, rect, offsets;  // per (view, Gaussian)
+    DevBuf scan_status;                    // frame kernel look-back words
+    DevBuf keys0, vals0, keys1, vals1;     // tile lists
+    DevBuf sort_hist, sort_status;
+    DevBuf ranges;
+    DevBuf counters;
+    DevBuf image;                          // images of the host-output variants
+    Counters* h_counters = nullptr;        // pinned mirror
+    ViewParams* h_views = nullptr;         // pinned staging
+    int h_views_cap = 0;
+    cudaEvent_t ev[8] = {};
+    int64_t key_capacity = 0;
+    int64_t per_view_capacity = 0;         // Gaussians * views the splat buffers hold
+};
+
+namespace {
+
+void make_view_params(const gs_camera& c, const gs_render_cfg& cfg, ViewParams& v)
+{
+    std::memcpy(v.view, c.view, sizeof(v.view));
+    std::memcpy(v.cam, c.position, sizeof(v.cam));
+    v.cot[0] = c.fov_cotangent[0];
+    v.cot[1] = c.fov_cotangent[1];
+    v.dsb[0] = c.depth_scale_bias[0];
+    v.dsb[1] = c.depth_scale_bias[1];
+    v.aspect = c.aspect;
+    v.width = c.width;
+    v.height = c.height;
+    v.tile_w = cfg.tile_w;
+    v.tile_h = cfg.tile_h;
+    v.tiles_x = (c.width + cfg.tile_w - 1) / cfg.tile_w;
+    v.tiles_y = (c.height + cfg.tile_h - 1) / cfg.tile_h;
+    v.tiles_xf = (float)c.width / (float)cfg.tile_w;
+    v.tiles_yf = (float)c.height / (float)cfg.tile_h;
+    v.tclip_x = ((float)cfg.tile_w / (float)c.width) * 2.0f;
+    v.tclip_y = ((float)cfg.tile_h / (float)c.height) * 2.0f;
+    v.texel_x = 2.0f / (float)c.width;
+    v.texel_y = 2.0f / (float)c.height;
+    // gaussian_render.cu:184-186: (1/pi) * texel * texel, per axis
+    const float k_Pi = 3.14159265359f;
+    v.bump_x = ((1.0f / k_Pi) * v.texel_x) * v.texel_x;
+    v.bump_y = ((1.0f / k_Pi) * v.texel_y) * v.texel_y;
+    v.tile_offset = 0;
+    v.out = nullptr;
+}
+
+bool valid_cfg(const gs_render_cfg& c)
+{
+    const bool shape = (c.tile_w == 16 && c.tile_h == 16) || (c.tile_w == 16 && c.tile_h == 8) ||
+                       (c.tile_w == 8 && c.tile_h == 8);
+    return shape && c.sh_max_degree >= 0 && c.sh_max_degree <= 3 &&
+           (c.termination == GS_TERM_REFERENCE || c.termination == GS_TERM_TMIN);
+}
+
+bool valid_cam(const gs_camera* c)
+{
+    return c && c->width > 0 && c->height > 0 && c->width <= 16384 && c->height <= 16384;
+}
+
+int eval_degree(const gs_scene* s, const gs_render_cfg& cfg) { return std::min(s->sh_degree, cfg.sh_max_degree); }
+
+float ms_between(cudaEvent_t a, cudaEvent_t b)
+{
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+int ensure_sort_scratch(gs_ctx* ctx, int64_t num_items)
+{
+    const int64_t tiles = (num_items + kSortTile - 1) / kSortTile;
+    if (ctx->sort_hist.ensure(sizeof(uint32_t) * kMaxPasses * kRadix) != cudaSuccess) return fail(GS_ERR_OOM, "sort hist");
+    const size_t need = sizeof(uint64_t) * (size_t)std::max<int64_t>(tiles, 1) * kRadix;
+    if (need > ctx->sort_status.bytes) {
+        // fresh words must read as unpublished for every epoch
+        if (ctx->sort_status.ensure(need, true) != cudaSuccess) return fail(GS_ERR_OOM, "sort status");
+    }
+    return GS_OK;
+}
+
+// Reserves `count` consecutive epochs of a look-back status array, clearing
+// the array when the 16-bit epoch would wrap.
+uint32_t take_epochs(uint32_t& epoch, uint32_t count, DevBuf& status, cudaStream_t st)
+{
+    if (epoch + count > 0xFFFFu) {
+        if (status.p) cudaMemsetAsync(status.p, 0, status.bytes, st);
+        epoch = 1;
+    }
+    const uint32_t e = epoch;
+    epoch += count;
+    return e;
+}
+
+int ensure_ctx_host(gs_ctx* ctx, int num_views)
+{
+    if (num_views > ctx->h_views_cap) {
+        if (ctx->h_views) cudaFreeHost(ctx->h_views);
+        ctx->h_views = nullptr;
+        GS_CUDA(cudaMallocHost(&ctx->h_views, sizeof(ViewParams) * (size_t)num_views));
+        ctx->h_views_cap = num_views;
+    }
+    if (ctx->views.ensure(sizeof(ViewParams) * (size_t)num_views) != cudaSuccess) return fail(GS_ERR_OOM, "views");
+    return GS_OK;
+}
+
+// One frame over `num_views` views of `scene`.  outs[v] receives view v.
+int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
+              uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
+{
+    if (!valid_cfg(cfg)) return fail(GS_ERR_INVALID, "invalid render cfg");
+    if (num_views <= 0) return fail(GS_ERR_INVALID, "no views");
+    for (int v = 0; v < num_views; ++v) {
+        if (!valid_cam(&cams[v])) return fail(GS_ERR_INVALID, "invalid camera");
+        if (!outs[v]) return fail(GS_ERR_INVALID, "null output");
+    }
+    GS_CUDA(cudaSetDevice(ctx->device));
+    int rc = ensure_ctx_host(ctx, num_views);
+    if (rc) return rc;
+
+    const int64_t n = scene->n;
+    int64_t tiles_total = 0;
+    for (int v = 0; v < num_views; ++v) {
+        ViewParams& vp = ctx->h_views[v];
+        make_view_params(cams[v], cfg, vp);
+        vp.tile_offset = tiles_total;
+        vp.out = reinterpret_cast<uchar4*>(outs[v]);
+        tiles_total += (int64_t)vp.tiles_x * vp.tiles_y;
+    }
+    if (tiles_total >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many tiles");
+    const int64_t items = n * num_views;
+    if (items >= (1ll << 31)) return fail(GS_ERR_INVALID, "views x Gaussians exceeds 2^31");
+    const int64_t groups = (n + 255) / 256;
+    const int64_t blocks = groups * num_views;
+
+    // per-(view, Gaussian) buffers
+    if (items > ctx->per_view_capacity) {
+        const size_t m = (size_t)items;
+        if (ctx->color.ensure(16 * m) || ctx->xy.ensure(8 * m) || ctx->z.ensure(4 * m) || ctx->ell.ensure(16 * m) ||
+            ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(8 * m))
+            return fail(GS_ERR_OOM, "splat buffers");
+        ctx->per_view_capacity = items;
+    }
+    if (sizeof(uint64_t) * (size_t)std::max<int64_t>(blocks, 1) > ctx->scan_status.bytes) {
+        if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(blocks, 1), true))
+            return fail(GS_ERR_OOM, "scan status");
+    }
+    if (ctx->ranges.ensure(sizeof(int32_t) * 2 * (size_t)tiles_total)) return fail(GS_ERR_OOM, "ranges");
+
+    Counters* dc = ctx->counters.as<Counters>();
+    GS_CUDA(cudaMemcpyAsync(ctx->views.p, ctx->h_views, sizeof(ViewParams) * num_views, cudaMemcpyHostToDevice, st));
+    GS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    GS_CUDA(cudaEventRecord(ctx->ev[0], st));
+
+    // 1. SH + projection + exact tile counts + key offsets
+    FrameArgs fa;
+    fa.n = n;
+    fa.num_views = num_views;
+    fa.epoch = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
+    fa.num_tiles = blocks;
+    fa.pos = scene->pos.as<float4>();
+    fa.sr = scene->sr.as<float4>();
+    fa.sh = scene->sh.as<float>();
+    fa.sh_count = scene->sh_count;
+    fa.color_in = scene->color.as<float4>();
+    fa.views = ctx->views.as<ViewParams>();
+    fa.color = ctx->color.as<float4>();
+    fa.xy = ctx->xy.as<float2>();
+    fa.z = ctx->z.as<float>();
+    fa.ell = ctx->ell.as<float4>();
+    fa.conic = ctx->conic.as<float4>();
+    fa.rect = ctx->rect.as<int2>();
+    fa.offsets = ctx->offsets.as<int64_t>();
+    fa.status = ctx->scan_status.as<uint64_t>();
+    fa.tile_counter = &dc->frame_tile;
+    fa.total = &dc->total;
+    fa.err = &dc->err;
+    // degree-0 scenes blend the model colours (ply_parser.cpp:383,389); SH
+    // scenes evaluate min(scene degree, cfg degree) (gaussian_render.cu:392)
+    if (scene->sh_degree == 0 && !scene->color.p) return fail(GS_ERR_INVALID, "scene has no colour");
+    const int deg = scene->sh_degree > 0 ? eval_degree(scene, cfg) : -1;
+    if (n > 0) launch_frame_project(fa, deg, st);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaEventRecord(ctx->ev[1], st));
+    GS_CUDA(cudaMemcpyAsync(ctx->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    GS_CUDA(cudaStreamSynchronize(st));
+    if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "projection look-back timed out");
+    const int64_t K = n > 0 ? ctx->h_counters->total : 0;
+    if (K >= (1ll << 31)) return fail(GS_ERR_CAPACITY, "more than 2^31 tile keys");
+
+    // 2. emit keys
+    if (K > ctx->key_capacity) {
+        if (ctx->keys0.ensure(8 * (size_t)K) || ctx->keys1.ensure(8 * (size_t)K) || ctx->vals0.ensure(4 * (size_t)K) ||
+            ctx->vals1.ensure(4 * (size_t)K))
+            return fail(GS_ERR_OOM, "tile lists");
+        ctx->key_capacity = (int64_t)(ctx->keys0.bytes / 8);
+    }
+    rc = ensure_sort_scratch(ctx, K);
+    if (rc) return rc;
+    GS_CUDA(cudaEventRecord(ctx->ev[2], st));
+    EmitArgs ea;
+    ea.n = n;
+    ea.num_views = num_views;
+    ea.views = ctx->views.as<ViewParams>();
+    ea.offsets = ctx->offsets.as<int64_t>();
+    ea.total = &dc->total;
+    ea.rect = ctx->rect.as<int2>();
+    ea.xy = ctx->xy.as<float2>();
+    ea.ell = ctx->ell.as<float4>();
+    ea.z = ctx->z.as<float>();
+    ea.keys = ctx->keys0.as<uint64_t>();
+    ea.values = ctx->vals0.as<int32_t>();
+    ea.capacity = ctx->key_capacity;
+    if (K > 0) launch_emit(ea, st);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaEventRecord(ctx->ev[3], st));
+
+    // 3. sort on the significant bits
+    const int key_bits = gs_key_bits(tiles_total);
+    SortScratch ss;
+    ss.hist = ctx->sort_hist.as<uint32_t>();
+    ss.status = ctx->sort_status.as<uint64_t>();
+    ss.counters = dc->sort_tiles;
+    ss.err = &dc->err;
+    ss.max_tiles = (int64_t)(ctx->sort_status.bytes / (8 * kRadix));
+    int passes = 0;
+    if (K > 0) {
+        const uint32_t ep = take_epochs(ctx->epoch_sort, (uint32_t)sort_passes(key_bits), ctx->sort_status, st);
+        passes = launch_sort(ctx->keys0.as<uint64_t>(), ctx->vals0.as<int32_t>(), ctx->keys1.as<uint64_t>(),
+                             ctx->vals1.as<int32_t>(), K, nullptr, key_bits, ss, ep, ctx->num_sms, st);
+    }
+    GS_CUDA(cudaGetLastError());
+    const uint64_t* skeys = (passes % 2) ? ctx->keys1.as<uint64_t>() : ctx->keys0.as<uint64_t>();
+    const int32_t* svals = (passes % 2) ? ctx->vals1.as<int32_t>() : ctx->vals0.as<int32_t>();
+    GS_CUDA(cudaEventRecord(ctx->ev[4], st));
+
+    // 4. tile ranges + raster
+    GS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0xFF, sizeof(int32_t) * 2 * (size_t)tiles_total, st));
+    if (K > 0) launch_ranges(skeys, K, nullptr, ctx->ranges.as<int32_t>(), st);
+    RasterArgs ra;
+    ra.view0 = ctx->h_views[0];
+    ra.views = ctx->views.as<ViewParams>();
+    ra.num_views = num_views;
+    ra.write_empty = 1;
+    ra.num_tiles_total = tiles_total;
+    ra.ranges = ctx->ranges.as<int32_t>();
+    ra.values = svals;
+    ra.xy = ctx->xy.as<float2>();
+    ra.conic = ctx->conic.as<float4>();
+    ra.color = ctx->color.as<float4>();
+    ra.t_min = cfg.t_min;
+    ra.tile_counter = &dc->raster_tile;
+    launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, num_views > 1, ctx->num_sms, st);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaEventRecord(ctx->ev[5], st));
+    GS_CUDA(cudaMemcpyAsync(&ctx->h_counters->err, &dc->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GS_CUDA(cudaStreamSynchronize(st));
+    if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "sort look-back timed out");
+
+    if (stats) {
+        stats->sh_eval_ms = 0.0;  // SH is fused into the projection kernel
+        stats->project_ms = ms_between(ctx->ev[0], ctx->ev[1]);
+        stats->build_tile_ms = ms_between(ctx->ev[2], ctx->ev[3]);
+        stats->sort_ms = ms_between(ctx->ev[3], ctx->ev[4]);
+        stats->raster_ms = ms_between(ctx->ev[4], ctx->ev[5]);
+        stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
+        stats->num_keys = K;
+        stats->num_tiles = tiles_total;
+        // frame kernel, emit, sort histogram + passes, ranges, raster
+        stats->kernel_launches = (n > 0 ? 1 : 0) + (K > 0 ? 3 + passes : 0) + 1;
+    }
+    return GS_OK;
+}
+
+}  // namespace
+
+// ============================================================================
+// C ABI
+// ============================================================================
+
+extern "C" {
+
+int gs_version(void) { return 100; }
+
+const char* gs_status_string(int status)
+{
+    switch (status) {
+        case GS_OK: return "ok";
+        case GS_ERR_INVALID: return "invalid argument";
+        case GS_ERR_OOM: return "out of device memory";
+        case GS_ERR_CAPACITY: return "buffer capacity exceeded";
+        case GS_ERR_DEVICE_TIMEOUT: return "bounded device wait timed out";
+        case GS_ERR_CUDA: return "CUDA error";
+        case GS_ERR_NO_DEVICE: return "no usable sm_100 device";
+        default: return "unknown status";
+    }
+}
+
+const char* gs_last_error_string(void) { return g_last_error.c_str(); }
+
+void gs_default_cfg(gs_render_cfg* cfg)
+{
+    if (!cfg) return;
+    cfg->sh_max_degree = 3;
+    cfg->termination = GS_TERM_TMIN;
+    cfg->t_min = 1e-4f;
+    cfg->tile_w = 16;
+    cfg->tile_h = 16;
+    cfg->raster_batch = 0;
+}
+
+void gs_camera_look_at(gs_camera* cam, const float eye[3], const float target[3], const float up[3], float fovy_rad,
+                       int32_t width, int32_t height, float znear, float zfar)
+{
+    if (!cam) return;
+    // glm::lookAtRH (ext/matrix_transform.inl:99-119)
+    float f[3] = {target[0] - eye[0], target[1] - eye[1], target[2] - eye[2]};
+    float fl = 1.0f / std::sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    for (float& x : f) x *= fl;
+    float s[3] = {f[1] * up[2] - f[2] * up[1], f[2] * up[0] - f[0] * up[2], f[0] * up[1] - f[1] * up[0]};
+    float sl = 1.0f / std::sqrt(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (float& x : s) x *= sl;
+    float u[3] = {s[1] * f[2] - s[2] * f[1], s[2] * f[0] - s[0] * f[2], s[0] * f[1] - s[1] * f[0]};
+    float* m = cam->view;
+    std::memset(m, 0, sizeof(cam->view));
+    m[0] = s[0];  m[4] = s[1];  m[8] = s[2];
+    m[1] = u[0];  m[5] = u[1];  m[9] = u[2];
+    m[2] = -f[0]; m[6] = -f[1]; m[10] = -f[2];
+    m[12] = -(s[0] * eye[0] + s[1] * eye[1] + s[2] * eye[2]);
+    m[13] = -(u[0] * eye[0] + u[1] * eye[1] + u[2] * eye[2]);
+    m[14] = (f[0] * eye[0] + f[1] * eye[1] + f[2] * eye[2]);
+    m[15] = 1.0f;
+    cam->position[0] = eye[0];
+    cam->position[1] = eye[1];
+    cam->position[2] = eye[2];
+    cam->width = width;
+    cam->height = height;
+    cam->aspect = (float)width / (float)height;
+    const float coty = 1.0f / std::tan(fovy_rad * 0.5f);
+    cam->fov_cotangent[0] = coty / cam->aspect;
+    cam->fov_cotangent[1] = coty;
+    cam->depth_scale_bias[0] = -2.0f / (zfar - znear);
+    cam->depth_scale_bias[1] = -(zfar + znear) / (zfar - znear);
+}
+
+int gs_ctx_create(int device, gs_ctx** out)
+{
+    if (!out) return fail(GS_ERR_INVALID, "out is null");
+    *out = nullptr;
+    int count = 0;
+    cudaError_t e = cudaGetDeviceCount(&count);
+    if (e != cudaSuccess || count <= device || device < 0) {
+        cudaGetLastError();
+        return fail(GS_ERR_NO_DEVICE, "no CUDA device");
+    }
+    cudaDeviceProp prop;
+    GS_CUDA(cudaGetDeviceProperties(&prop, device));
+    if (prop.major != 10 || prop.minor != 0) return fail(GS_ERR_NO_DEVICE, "device is not sm_100 (B200)");
+    GS_CUDA(cudaSetDevice(device));
+    gs_ctx* c = new (std::nothrow) gs_ctx();
+    if (!c) return fail(GS_ERR_OOM, "host allocation");
+    c->device = device;
+    c->num_sms = prop.multiProcessorCount;
+    if (c->counters.ensure(sizeof(Counters), true) != cudaSuccess) {
+        delete c;
+        return fail(GS_ERR_OOM, "counters");
+    }
+    if (cudaMallocHost(&c->h_counters, sizeof(Counters)) != cudaSuccess) {
+        c->counters.release();
+        delete c;
+        return fail(GS_ERR_OOM, "pinned counters");
+    }
+    for (auto& ev : c->ev) cudaEventCreate(&ev);
+    *out = c;
+    return GS_OK;
+}
+
+int gs_ctx_destroy(gs_ctx* ctx)
+{
+    if (!ctx) return GS_OK;
+    cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
+                      &ctx->offsets, &ctx->scan_status, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
+                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
+    for (DevBuf* b : bufs) b->release();
+    if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+    if (ctx->h_views) cudaFreeHost(ctx->h_views);
+    for (auto& ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    delete ctx;
+    return GS_OK;
+}
+
+int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
+{
+    if (!ctx) return 0;
+    const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
+                            &ctx->offsets, &ctx->scan_status, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
+                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
+    int64_t t = 0;
+    for (const DevBuf* b : bufs) t += (int64_t)b->bytes;
+    return t;
+}
+
+int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
+                    const float* h_color, const float* h_sh, int32_t sh_degree, gs_scene** out)
+{
+    if (!ctx || !out || n < 0 || !h_position || !h_scale_rotation) return fail(GS_ERR_INVALID, "null argument");
+    if (sh_degree < 0 || sh_degree > 3) return fail(GS_ERR_INVALID, "sh_degree must be 0..3");
+    if (sh_degree > 0 && !h_sh) return fail(GS_ERR_INVALID, "SH scene without coefficients");
+    if (sh_degree == 0 && !h_color) return fail(GS_ERR_INVALID, "degree-0 scene without colours");
+    if (n >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many Gaussians");
+    *out = nullptr;
+    GS_CUDA(cudaSetDevice(ctx->device));
+    gs_scene* s = new (std::nothrow) gs_scene();
+    if (!s) return fail(GS_ERR_OOM, "host allocation");
+    s->device = ctx->device;
+    s->n = n;
+    s->sh_degree = sh_degree;
+    s->sh_count = 3 * (sh_degree + 1) * (sh_degree + 1);
+    const size_t m = (size_t)std::max<int64_t>(n, 1);
+    const size_t groups = (size_t)((n + 255) / 256);
+    bool ok = s->pos.ensure(16 * m) == cudaSuccess && s->sr.ensure(16 * m) == cudaSuccess;
+    if (ok && h_color) ok = s->color.ensure(16 * m) == cudaSuccess;
+    if (ok && sh_degree > 0) ok = s->sh.ensure(sizeof(float) * std::max<size_t>(groups, 1) * 256 * s->sh_count) == cudaSuccess;
+    if (!ok) {
+        gs_scene_destroy(s);
+        return fail(GS_ERR_OOM, "scene buffers");
+    }
+    cudaError_t e = cudaMemcpy(s->pos.p, h_position, 16 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(s->sr.p, h_scale_rotation, 16 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && h_color) e = cudaMemcpy(s->color.p, h_color, 16 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && sh_degree > 0)
+        e = cudaMemcpy(s->sh.p, h_sh, sizeof(float) * groups * 256 * s->sh_count, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        gs_scene_destroy(s);
+        return cuda_fail(e, "scene upload");
+    }
+    *out = s;
+    return GS_OK;
+}
+
+int gs_scene_destroy(gs_scene* s)
+{
+    if (!s) return GS_OK;
+    cudaSetDevice(s->device);
+    s->pos.release();
+    s->sr.release();
+    s->color.release();
+    s->sh.release();
+    delete s;
+    return GS_OK;
+}
+
+int64_t gs_scene_size(const gs_scene* s) { return s ? s->n : 0; }
+
+int64_t gs_scene_device_bytes(const gs_scene* s)
+{
+    return s ? (int64_t)(s->pos.bytes + s->sr.bytes + s->color.bytes + s->sh.bytes) : 0;
+}
+
+int gs_render(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cam, const gs_render_cfg* cfg, uint8_t* d_rgba,
+              gs_stats* stats, void* stream)
+{
+    if (!ctx || !scene || !cam || !cfg || !d_rgba) return fail(GS_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    uint8_t* outs[1] = {d_rgba};
+    return run_frame(ctx, scene, cam, 1, *cfg, outs, stats, (cudaStream_t)stream);
+}
+
+int gs_render_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cam, const gs_render_cfg* cfg,
+                   uint8_t* h_rgba, gs_stats* stats, void* stream)
+{
+    if (!ctx || !scene || !cam || !cfg || !h_rgba) return fail(GS_ERR_INVALID, "null argument");
+    if (!valid_cam(cam)) return fail(GS_ERR_INVALID, "invalid camera");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    const size_t bytes = 4 * (size_t)cam->width * cam->height;
+    if (ctx->image.ensure(bytes)) return fail(GS_ERR_OOM, "image");
+    uint8_t* outs[1] = {ctx->image.as<uint8_t>()};
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = run_frame(ctx, scene, cam, 1, *cfg, outs, stats, st);
+    if (rc) return rc;
+    GS_CUDA(cudaMemcpyAsync(h_rgba, ctx->image.p, bytes, cudaMemcpyDeviceToHost, st));
+    GS_CUDA(cudaStreamSynchronize(st));
+    return GS_OK;
+}
+
+int gs_render_batch(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                    const gs_render_cfg* cfg, uint8_t* const* d_rgba, gs_stats* stats, void* stream)
+{
+    if (!ctx || !scene || !cams || !cfg || !d_rgba || num_views <= 0) return fail(GS_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    return run_frame(ctx, scene, cams, num_views, *cfg, d_rgba, stats, (cudaStream_t)stream);
+}
+
+int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                         const gs_render_cfg* cfg, uint8_t* h_rgba, gs_stats* stats, void* stream)
+{
+    if (!ctx || !scene || !cams || !cfg || !h_rgba || num_views <= 0) return fail(GS_ERR_INVALID, "null argument");
+    for (int v = 0; v < num_views; ++v)
+        if (!valid_cam(&cams[v])) return fail(GS_ERR_INVALID, "invalid camera");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    size_t total = 0;
+    std::vector<size_t> offs((size_t)num_views);
+    for (int v = 0; v < num_views; ++v) {
+        offs[v] = total;
+        total += 4 * (size_t)cams[v].width * cams[v].height;
+    }
+    if (ctx->image.ensure(total)) return fail(GS_ERR_OOM, "image");
+    std::vector<uint8_t*> outs((size_t)num_views);
+    for (int v = 0; v < num_views; ++v) outs[v] = ctx->image.as<uint8_t>() + offs[v];
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = run_frame(ctx, scene, cams, num_views, *cfg, outs.data(), stats, st);
+    if (rc) return rc;
+    GS_CUDA(cudaMemcpyAsync(h_rgba, ctx->image.p, total, cudaMemcpyDeviceToHost, st));
+    GS_CUDA(cudaStreamSynchronize(st));
+    return GS_OK;
+}
+
+// ---- stage API ----------------------------------------------------------------
+
+int gs_stage_sh(int64_t n, const float* d_position, const float* d_sh, int32_t sh_count, int32_t eval_degree,
+                const gs_camera* cam, float* d_color, void* stream)
+{
+    if (n < 0 || !cam || (n > 0 && (!d_position || !d_sh || !d_color))) return fail(GS_ERR_INVALID, "null argument");
+    if (eval_degree < 0 || eval_degree > 3 || sh_count < 3 * (eval_degree + 1) * (eval_degree + 1))
+        return fail(GS_ERR_INVALID, "bad SH degree/count");
+    gs_render_cfg cfg;
+    gs_default_cfg(&cfg);
+    ViewParams v;
+    make_view_params(*cam, cfg, v);
+    launch_sh_stage(n, (const float4*)d_position, d_sh, sh_count, eval_degree, v, (float4*)d_color,
+                    (cudaStream_t)stream);
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
+int gs_stage_project(int64_t n, const float* d_position, const float* d_scale_rotation, const gs_camera* cam,
+                     float* d_xy, float* d_z, float* d_ellipse, float* d_conic, void* stream)
+{
+    if (n < 0 || !valid_cam(cam)) return fail(GS_ERR_INVALID, "bad argument");
+    if (n > 0 && (!d_position || !d_scale_rotation || !d_xy || !d_z || !d_ellipse || !d_conic))
+        return fail(GS_ERR_INVALID, "null argument");
+    gs_render_cfg cfg;
+    gs_default_cfg(&cfg);
+    ViewParams v;
+    make_view_params(*cam, cfg, v);
+    launch_project_stage(n, (const float4*)d_position, (const float4*)d_scale_rotation, v, (float2*)d_xy, d_z,
+                         (float4*)d_ellipse, (float4*)d_conic, (cudaStream_t)stream);
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
+int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, const float* d_ellipse,
+                   const gs_camera* cam, const gs_render_cfg* cfg, uint64_t* d_keys, int32_t* d_values,
+                   int64_t capacity, int64_t* out_num_keys, void* stream)
+{
+    if (!ctx || !cfg || !valid_cam(cam) || n < 0 || !out_num_keys) return fail(GS_ERR_INVALID, "bad argument");
+    if (!valid_cfg(*cfg)) return fail(GS_ERR_INVALID, "invalid render cfg");
+    if (n >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many Gaussians");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    *out_num_keys = 0;
+    if (n == 0) return GS_OK;
+    int rc = ensure_ctx_host(ctx, 1);
+    if (rc) return rc;
+    ViewParams& v = ctx->h_views[0];
+    make_view_params(*cam, *cfg, v);
+    const int64_t blocks = (n + 255) / 256;
+    if (ctx->rect.ensure(8 * (size_t)n) || ctx->offsets.ensure(8 * (size_t)n)) return fail(GS_ERR_OOM, "build buffers");
+    ctx->per_view_capacity = 0;  // rect/offsets may have been regrown: force the frame path to re-check
+    if (sizeof(uint64_t) * (size_t)blocks > ctx->scan_status.bytes) {
+        if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)blocks, true)) return fail(GS_ERR_OOM, "scan status");
+    }
+    Counters* dc = ctx->counters.as<Counters>();
+    GS_CUDA(cudaMemcpyAsync(ctx->views.p, &v, sizeof(ViewParams), cudaMemcpyHostToDevice, st));
+    GS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    FrameArgs fa = {};
+    fa.n = n;
+    fa.num_views = 1;
+    fa.epoch = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
+    fa.num_tiles = blocks;
+    fa.views = ctx->views.as<ViewParams>();
+    fa.xy = (float2*)d_xy;
+    fa.ell = (float4*)d_ellipse;
+    fa.rect = ctx->rect.as<int2>();
+    fa.offsets = ctx->offsets.as<int64_t>();
+    fa.status = ctx->scan_status.as<uint64_t>();
+    fa.tile_counter = &dc->frame_tile;
+    fa.total = &dc->total;
+    fa.err = &dc->err;
+    launch_count_stage(fa, st);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaMemcpyAsync(ctx->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    GS_CUDA(cudaStreamSynchronize(st));
+    if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "build look-back timed out");
+    const int64_t K = ctx->h_counters->total;
+    *out_num_keys = K;
+    if (K > capacity) return fail(GS_ERR_CAPACITY, "tile list capacity exceeded");
+    if (K > 0 && (!d_keys || !d_values)) return fail(GS_ERR_INVALID, "null key buffers");
+    EmitArgs ea;
+    ea.n = n;
+    ea.num_views = 1;
+    ea.views = ctx->views.as<ViewParams>();
+    ea.offsets = ctx->offsets.as<int64_t>();
+    ea.total = &dc->total;
+    ea.rect = ctx->rect.as<int2>();
+    ea.xy = (const float2*)d_xy;
+    ea.ell = (const float4*)d_ellipse;
+    ea.z = d_z;
+    ea.keys = d_keys;
+    ea.values = d_values;
+    ea.capacity = capacity;
+    if (K > 0) launch_emit(ea, st);
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
+int gs_stage_sort(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, uint64_t* d_keys, int32_t* d_values,
+                  uint64_t* d_keys_alt, int32_t* d_values_alt, int32_t* out_selector, void* stream)
+{
+    if (!ctx || !out_selector || num_keys < 0 || key_bits < 1 || key_bits > 64) return fail(GS_ERR_INVALID, "bad argument");
+    if (num_keys >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many keys");
+    *out_selector = 0;
+    if (num_keys == 0) return GS_OK;
+    if (!d_keys || !d_values || !d_keys_alt || !d_values_alt) return fail(GS_ERR_INVALID, "null buffer");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ensure_sort_scratch(ctx, num_keys);
+    if (rc) return rc;
+    Counters* dc = ctx->counters.as<Counters>();
+    GS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+    SortScratch ss;
+    ss.hist = ctx->sort_hist.as<uint32_t>();
+    ss.status = ctx->sort_status.as<uint64_t>();
+    ss.counters = dc->sort_tiles;
+    ss.err = &dc->err;
+    ss.max_tiles = (int64_t)(ctx->sort_status.bytes / (8 * kRadix));
+    const uint32_t ep = take_epochs(ctx->epoch_sort, (uint32_t)sort_passes(key_bits), ctx->sort_status, st);
+    const int passes =
+        launch_sort(d_keys, d_values, d_keys_alt, d_values_alt, num_keys, nullptr, key_bits, ss, ep, ctx->num_sms, st);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(cudaMemcpyAsync(&ctx->h_counters->err, &dc->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    GS_CUDA(cudaStreamSynchronize(st));
+    if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "sort look-back timed out");
+    *out_selector = passes % 2;
+    return GS_OK;
+}
+
+int gs_stage_ranges(int64_t num_keys, const uint64_t* d_keys, int64_t num_tiles, int32_t* d_ranges, void* stream)
+{
+    if (num_keys < 0 || num_tiles <= 0 || !d_ranges || (num_keys > 0 && !d_keys)) return fail(GS_ERR_INVALID, "bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    GS_CUDA(cudaMemsetAsync(d_ranges, 0xFF, sizeof(int32_t) * 2 * (size_t)num_tiles, st));
+    if (num_keys > 0) launch_ranges(d_keys, num_keys, nullptr, d_ranges, st);
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
+int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_t* d_ranges, const int32_t* d_values,
+                    const float* d_xy, const float* d_conic, const float* d_color, uint8_t* d_rgba, void* stream)
+{
+    if (!valid_cam(cam) || !cfg || !d_ranges || !d_rgba) return fail(GS_ERR_INVALID, "bad argument");
+    if (!valid_cfg(*cfg)) return fail(GS_ERR_INVALID, "invalid render cfg");
+    RasterArgs ra = {};
+    make_view_params(*cam, *cfg, ra.view0);
+    ra.view0.out = reinterpret_cast<uchar4*>(d_rgba);
+    ra.views = nullptr;
+    ra.num_views = 1;
+    ra.write_empty = 0;
+    ra.num_tiles_total = (int64_t)ra.view0.tiles_x * ra.view0.tiles_y;
+    ra.ranges = d_ranges;
+    ra.values = d_values;
+    ra.xy = (const float2*)d_xy;
+    ra.conic = (const float4*)d_conic;
+    ra.color = (const float4*)d_color;
+    ra.t_min = cfg->t_min;
+    launch_raster(ra, cfg->tile_w, cfg->tile_h, cfg->termination, false, 148, (cudaStream_t)stream);
+    GS_CUDA(cudaGetLastError());
+    return GS_OK;
+}
+
+int64_t gs_num_tiles(int32_t width, int32_t height, const gs_render_cfg* cfg)
+{
+    if (!cfg || width <= 0 || height <= 0 || cfg->tile_w <= 0 || cfg->tile_h <= 0) return 0;
+    return (int64_t)((width + cfg->tile_w - 1) / cfg->tile_w) * ((height + cfg->tile_h - 1) / cfg->tile_h);
+}
+
+int32_t gs_key_bits(int64_t num_tiles)
+{
+    int32_t bits = 0;
+    while (bits < 31 && (1ll << bits) < num_tiles) ++bits;
+    return 32 + bits;
+}
+
+}  // extern "C"

@@ -1,0 +1,104 @@
+// Kernel argument blocks and launchers of the gs_b200 pipeline (internal).
+#pragma once
+
+#include "gs_common.cuh"
+
+namespace gs {
+
+constexpr int kErrTimeout = 4;  // GS_ERR_DEVICE_TIMEOUT
+
+// Fused SH + projection + count + scan over (view, Gaussian) pairs.
+struct FrameArgs {
+    int64_t n;          // Gaussians per view
+    int32_t num_views;
+    uint32_t epoch;     // look-back epoch of this launch
+    int64_t num_tiles;  // blocks = num_views * ceil(n / 256)
+    const float4* pos;
+    const float4* sr;
+    const float* sh;    // grouped [ceil(n/256)][sh_count][256]
+    int32_t sh_count;
+    const float4* color_in;  // degree-0 scenes: colour from the model
+    const ViewParams* views;
+    // outputs, per view at [view * n + i]
+    float4* color;
+    float2* xy;
+    float* z;
+    float4* ell;
+    float4* conic;
+    int2* rect;
+    int64_t* offsets;
+    // scratch
+    uint64_t* status;   // num_tiles words
+    unsigned long long* tile_counter;
+    int64_t* total;
+    int* err;
+};
+
+struct EmitArgs {
+    int64_t n;
+    int32_t num_views;
+    const ViewParams* views;
+    const int64_t* offsets;
+    const int64_t* total;
+    const int2* rect;
+    const float2* xy;
+    const float4* ell;
+    const float* z;
+    uint64_t* keys;
+    int32_t* values;
+    int64_t capacity;
+};
+
+// Onesweep LSD radix sort of (uint64 key, int32 value) pairs.
+constexpr int kSortThreads = 256;
+constexpr int kSortIpt = 16;
+constexpr int kSortTile = kSortThreads * kSortIpt;
+constexpr int kRadix = 256;
+constexpr int kMaxPasses = 8;
+
+struct SortScratch {
+    uint32_t* hist;                   // [kMaxPasses][kRadix]
+    uint64_t* status;                 // [max_tiles][kRadix] look-back words, reused by every pass
+    unsigned long long* counters;     // [kMaxPasses] tile counters
+    int* err;
+    int64_t max_tiles;
+};
+
+struct RasterArgs {
+    ViewParams view0;                 // single-view kernel: the view, by value
+    const ViewParams* views;          // persistent kernel: all views
+    int32_t num_views;
+    int32_t write_empty;              // 1: tiles without entries are written as (0,0,0,0)
+    int64_t num_tiles_total;          // sum of the views' tiles
+    const int32_t* ranges;            // [2 * num_tiles_total]
+    const int32_t* values;
+    const float2* xy;                 // indexed by value
+    const float4* conic;
+    const float4* color;
+    float t_min;
+    unsigned long long* tile_counter; // persistent variant only
+};
+
+void launch_sh_stage(int64_t n, const float4* pos, const float* sh, int sh_count, int deg, const ViewParams& v,
+                     float4* color, cudaStream_t st);
+void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const ViewParams& v, float2* xy,
+                          float* z, float4* ell, float4* conic, cudaStream_t st);
+void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st);
+void launch_count_stage(const FrameArgs& a, cudaStream_t st);
+void launch_emit(const EmitArgs& a, cudaStream_t st);
+
+// Sorts num_items pairs on bits [0, key_bits).  When d_num_items is non-null
+// the item count is read on the device (graph-friendly; num_items is then
+// an upper bound used to size the grids).  Returns the number of passes;
+// the result is in the alternate buffers when that number is odd.
+int launch_sort(const uint64_t* keys_in, const int32_t* vals_in, uint64_t* keys_alt, int32_t* vals_alt,
+                int64_t num_items, const int64_t* d_num_items, int key_bits, const SortScratch& s, uint32_t epoch,
+                int num_sms, cudaStream_t st);
+int sort_passes(int key_bits);
+
+void launch_ranges(const uint64_t* keys, int64_t num_items, const int64_t* d_num_items, int32_t* ranges,
+                   cudaStream_t st);
+void launch_raster(const RasterArgs& a, int tile_w, int tile_h, int termination, bool persistent, int num_sms,
+                   cudaStream_t st);
+
+}  // namespace gs

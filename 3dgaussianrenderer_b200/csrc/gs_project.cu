@@ -1,0 +1,372 @@
+// Per-Gaussian kernels of the gs_b200 pipeline:
+//   * stage kernels with the reference's buffer layouts (SH only,
+//     projection only), used by the stage API;
+//   * the fused frame kernel: SH colour + EWA projection + tile rectangle +
+//     exact per-Gaussian overlap count (warp-cooperative) + single-pass
+//     decoupled look-back scan of the counts into key offsets;
+//   * the emit kernel that writes (tile|depth, index) keys at those offsets.
+#include "gs_kernels.h"
+
+namespace gs {
+
+// ---- stage kernels (reference layouts) -------------------------------------
+
+template <int DEG>
+__global__ void __launch_bounds__(256) sh_stage_kernel(int64_t n, const float4* __restrict__ pos,
+                                                       const float* __restrict__ sh, int sh_count,
+                                                       const ViewParams v, float4* __restrict__ color)
+{
+    // The grouped SH layout is [group of 256][coefficient][256]; with one
+    // Gaussian per thread and 256-thread blocks every coefficient load of a
+    // warp is one contiguous 128-byte line (gaussian_render.cu:109-112).
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = __ldg(&pos[i]);
+    const float3 d = view_dir(v, p);
+    const float* base = sh + (int64_t)blockIdx.x * 256 * sh_count + threadIdx.x;
+    const float3 c = sh_color<DEG>(d.x, d.y, d.z, base, 256);
+    color[i] = make_float4(c.x, c.y, c.z, p.w);
+}
+
+__global__ void __launch_bounds__(256) project_stage_kernel(int64_t n, const float4* __restrict__ pos,
+                                                            const float4* __restrict__ sr,
+                                                            const ViewParams v, float2* __restrict__ xy,
+                                                            float* __restrict__ z, float4* __restrict__ ell,
+                                                            float4* __restrict__ conic)
+{
+    const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
+    if (i >= n) return;
+    const Splat s = project_gaussian(__ldg(&pos[i]), __ldg(&sr[i]), v);
+    xy[i] = make_float2(s.x, s.y);
+    z[i] = s.z;
+    ell[i] = make_float4(s.cs, s.sn, s.ex, s.ey);
+    conic[i] = make_float4(s.ca, s.cb, s.cc, 0.0f);
+}
+
+// ---- warp-cooperative overlap counting -------------------------------------
+//
+// Each lane owns one Gaussian with `cand` candidate tiles.  The warp walks
+// the concatenation of its 32 candidate lists 32 candidates at a time, so
+// one huge splat does not serialise its lane: lane l tests candidate
+// base + l of whichever Gaussian owns it (found by a 5-step search over the
+// warp's inclusive scan).
+
+struct WarpCands {
+    int incl, excl, total;
+};
+
+__device__ __forceinline__ WarpCands warp_scan_cands(const int cand)
+{
+    const int lane = threadIdx.x & 31;
+    int incl = cand;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    WarpCands w;
+    w.incl = incl;
+    w.excl = incl - cand;
+    w.total = __shfl_sync(kFull, incl, 31);
+    return w;
+}
+
+__device__ __forceinline__ int owner_of(const int incl, const int c)
+{
+    int pos = 0;
+#pragma unroll
+    for (int b = 16; b >= 1; b >>= 1) {
+        const int t = __shfl_sync(kFull, incl, pos + b - 1);
+        if (t <= c) pos += b;
+    }
+    return pos;
+}
+
+__device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
+{
+    if (hi <= lo) return 0u;
+    const unsigned mhi = hi >= 32 ? kFull : ((1u << hi) - 1u);
+    const unsigned mlo = (1u << lo) - 1u;
+    return mhi & ~mlo;
+}
+
+__device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v)
+{
+    const int lane = threadIdx.x & 31;
+    const WarpCands w = warp_scan_cands(cand);
+    int hits = 0;
+    for (int base = 0; base < w.total; base += 32) {
+        const int c = base + lane;
+        const int o = owner_of(w.incl, c);
+        Ell oe;
+        oe.cx = __shfl_sync(kFull, e.cx, o);
+        oe.cy = __shfl_sync(kFull, e.cy, o);
+        oe.cs = __shfl_sync(kFull, e.cs, o);
+        oe.sn = __shfl_sync(kFull, e.sn, o);
+        oe.ex = __shfl_sync(kFull, e.ex, o);
+        oe.ey = __shfl_sync(kFull, e.ey, o);
+        int4 orr;
+        orr.x = __shfl_sync(kFull, r.x, o);
+        orr.y = __shfl_sync(kFull, r.y, o);
+        orr.z = __shfl_sync(kFull, r.z, o);
+        orr.w = __shfl_sync(kFull, r.w, o);
+        const int oexcl = __shfl_sync(kFull, w.excl, o);
+        bool hit = false;
+        if (c < w.total) {
+            int tile;
+            hit = candidate_hit(oe, orr, c - oexcl, v, tile);
+        }
+        const unsigned bal = __ballot_sync(kFull, hit);
+        hits += __popc(bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32)));
+    }
+    return hits;
+}
+
+// ---- block scan + decoupled look-back over blocks ----------------------------
+
+// Returns this thread's exclusive offset among all threads of all blocks
+// (ordered by dynamic block id), writes the grand total when last.
+__device__ __forceinline__ int64_t block_offsets(const int hits, const int64_t tile, const int64_t num_tiles,
+                                                 uint64_t* status, const uint32_t epoch, int64_t* total_out, int* err)
+{
+    __shared__ int s_warp[8];
+    __shared__ int64_t s_base;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int incl = hits;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int k = 0; k < 8; ++k) {
+            const int t = s_warp[k];
+            s_warp[k] = run;
+            run += t;
+        }
+        const uint64_t agg = (uint64_t)run;
+        uint64_t excl = 0;
+        if (tile == 0) {
+            store_status(status, status_word(kFlagP, epoch, agg));
+        } else {
+            store_status(status + tile, status_word(kFlagA, epoch, agg));
+            excl = look_back(status, tile, 1, epoch, err, kErrTimeout);
+            store_status(status + tile, status_word(kFlagP, epoch, excl + agg));
+        }
+        s_base = (int64_t)excl;
+        if (tile == num_tiles - 1) *total_out = (int64_t)(excl + agg);
+    }
+    __syncthreads();
+    return s_base + s_warp[warp] + (incl - hits);
+}
+
+__device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
+{
+    __shared__ int64_t s_tile;
+    if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(counter, 1ull);
+    __syncthreads();
+    return s_tile;
+}
+
+// ---- fused frame kernel ------------------------------------------------------
+//
+// One 256-thread block per (view, group of 256 Gaussians), blocks taken in
+// a dynamic order so the look-back never waits on an unscheduled block.
+// Per Gaussian it reads position, scale/rotation and (DEG >= 0) the group's
+// SH coefficients (DEG = -1: degree-0 scene, colour copied from the model), and writes colour, clip centre, depth, ellipse, conic,
+// packed tile rectangle and the exclusive key offset.
+template <int DEG>
+__global__ void __launch_bounds__(256) frame_project_kernel(FrameArgs a)
+{
+    const int64_t tile = acquire_tile(a.tile_counter);
+    const int64_t groups = (a.n + 255) / 256;
+    const int view = (int)(tile / groups);
+    const int64_t group = tile - (int64_t)view * groups;
+    const int64_t i = group * 256 + threadIdx.x;
+    const bool valid = i < a.n;
+    const ViewParams& v = a.views[view];
+    const int64_t o = (int64_t)view * a.n + i;  // per-view output index
+
+    Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int4 r = make_int4(0, 0, 0, 0);
+    int cand = 0;
+    if (valid) {
+        const float4 p = __ldg(&a.pos[i]);
+        const float4 sr = __ldg(&a.sr[i]);
+        if (DEG >= 0) {
+            const float3 d = view_dir(v, p);
+            const float3 c = sh_color<DEG>(d.x, d.y, d.z, a.sh + group * 256 * a.sh_count + threadIdx.x, 256);
+            a.color[o] = make_float4(c.x, c.y, c.z, p.w);
+        } else {
+            a.color[o] = __ldg(&a.color_in[i]);
+        }
+        const Splat s = project_gaussian(p, sr, v);
+        a.xy[o] = make_float2(s.x, s.y);
+        a.z[o] = s.z;
+        a.ell[o] = make_float4(s.cs, s.sn, s.ex, s.ey);
+        a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
+        e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
+        r = tile_rect(e, v);
+        cand = rect_candidates(r);
+        a.rect[o] = pack_rect(r);
+    }
+    const int hits = warp_count_hits(e, r, cand, v);
+    const int64_t off = block_offsets(hits, tile, a.num_tiles, a.status, a.epoch, a.total, a.err);
+    if (valid) a.offsets[o] = off;
+}
+
+// Count-only variant for the stage API: rectangle + exact count + scan from
+// already projected (xy, ellipse) in the reference layouts.
+__global__ void __launch_bounds__(256) count_stage_kernel(FrameArgs a)
+{
+    const int64_t tile = acquire_tile(a.tile_counter);
+    const int64_t i = tile * 256 + threadIdx.x;
+    const bool valid = i < a.n;
+    const ViewParams& v = a.views[0];
+    Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    int4 r = make_int4(0, 0, 0, 0);
+    int cand = 0;
+    if (valid) {
+        const float2 c = __ldg(&a.xy[i]);
+        const float4 el = __ldg(&a.ell[i]);
+        e = {c.x, c.y, el.x, el.y, el.z, el.w};
+        r = tile_rect(e, v);
+        cand = rect_candidates(r);
+        a.rect[i] = pack_rect(r);
+    }
+    const int hits = warp_count_hits(e, r, cand, v);
+    const int64_t off = block_offsets(hits, tile, a.num_tiles, a.status, a.epoch, a.total, a.err);
+    if (valid) a.offsets[i] = off;
+}
+
+// ---- emit -------------------------------------------------------------------
+//
+// Rewalks each warp's candidates and writes every hit at
+// offsets[g] + (number of earlier hits of g), so keys leave in Gaussian
+// order with tiles ascending inside a Gaussian; a stable sort then breaks
+// equal keys by index.  The key holds the global tile id (view tile offset
+// + tile) and the value the per-view-flattened Gaussian index.
+__global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
+{
+    const int64_t gi = (int64_t)blockIdx.x * 256 + threadIdx.x;  // over views * n
+    const int64_t total_items = (int64_t)a.num_views * a.n;
+    const bool valid = gi < total_items;
+    // a warp may straddle two views; every owner's view travels with it
+    const int view = valid ? (int)(gi / a.n) : 0;
+    const int lane = threadIdx.x & 31;
+
+    int cand = 0, hits = 0;
+    int4 r = make_int4(0, 0, 0, 0);
+    Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    float depth = 0.f;
+    int64_t off = 0;
+    if (valid) {
+        off = a.offsets[gi];
+        const int64_t next = (gi + 1 < total_items) ? a.offsets[gi + 1] : *a.total;
+        hits = (int)(next - off);
+        if (hits > 0) {
+            r = unpack_rect(a.rect[gi]);
+            cand = rect_candidates(r);
+            const float2 c = a.xy[gi];
+            const float4 el = a.ell[gi];
+            e = {c.x, c.y, el.x, el.y, el.z, el.w};
+            depth = a.z[gi];
+        }
+    }
+    if (__ballot_sync(kFull, cand > 0) == 0) return;
+    const WarpCands w = warp_scan_cands(cand);
+    int running = 0;
+    for (int base = 0; base < w.total; base += 32) {
+        const int c = base + lane;
+        const int o = owner_of(w.incl, c);
+        Ell oe;
+        oe.cx = __shfl_sync(kFull, e.cx, o);
+        oe.cy = __shfl_sync(kFull, e.cy, o);
+        oe.cs = __shfl_sync(kFull, e.cs, o);
+        oe.sn = __shfl_sync(kFull, e.sn, o);
+        oe.ex = __shfl_sync(kFull, e.ex, o);
+        oe.ey = __shfl_sync(kFull, e.ey, o);
+        int4 orr;
+        orr.x = __shfl_sync(kFull, r.x, o);
+        orr.y = __shfl_sync(kFull, r.y, o);
+        orr.z = __shfl_sync(kFull, r.z, o);
+        orr.w = __shfl_sync(kFull, r.w, o);
+        const int oexcl = __shfl_sync(kFull, w.excl, o);
+        const int oincl = __shfl_sync(kFull, w.incl, o);
+        const int orun = __shfl_sync(kFull, running, o);
+        const float oz = __shfl_sync(kFull, depth, o);
+        const long long ooff = __shfl_sync(kFull, (long long)off, o);
+        const int oview = __shfl_sync(kFull, view, o);
+        bool hit = false;
+        int tile = 0;
+        if (c < w.total) hit = candidate_hit(oe, orr, c - oexcl, a.views[oview], tile);
+        const unsigned bal = __ballot_sync(kFull, hit);
+        if (hit) {
+            const unsigned omask = lane_range_mask(max(oexcl - base, 0), min(oincl - base, 32));
+            const int rank = __popc(bal & omask & lanemask_lt());
+            const int64_t dst = ooff + orun + rank;
+            if (dst < a.capacity) {
+                const int64_t gtile = a.views[oview].tile_offset + tile;
+                a.keys[dst] = make_key((uint64_t)gtile, oz);
+                a.values[dst] = (int32_t)((int64_t)blockIdx.x * 256 + (threadIdx.x & ~31) + o);
+            }
+        }
+        running += __popc(bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32)));
+    }
+}
+
+// ---- launchers ----------------------------------------------------------------
+
+void launch_sh_stage(int64_t n, const float4* pos, const float* sh, int sh_count, int deg, const ViewParams& v,
+                     float4* color, cudaStream_t st)
+{
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (grid == 0) return;
+    switch (deg) {
+        case 0: sh_stage_kernel<0><<<grid, 256, 0, st>>>(n, pos, sh, sh_count, v, color); break;
+        case 1: sh_stage_kernel<1><<<grid, 256, 0, st>>>(n, pos, sh, sh_count, v, color); break;
+        case 2: sh_stage_kernel<2><<<grid, 256, 0, st>>>(n, pos, sh, sh_count, v, color); break;
+        default: sh_stage_kernel<3><<<grid, 256, 0, st>>>(n, pos, sh, sh_count, v, color); break;
+    }
+}
+
+void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const ViewParams& v, float2* xy,
+                          float* z, float4* ell, float4* conic, cudaStream_t st)
+{
+    const unsigned grid = (unsigned)((n + 255) / 256);
+    if (grid == 0) return;
+    project_stage_kernel<<<grid, 256, 0, st>>>(n, pos, sr, v, xy, z, ell, conic);
+}
+
+void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st)
+{
+    const unsigned grid = (unsigned)a.num_tiles;
+    if (grid == 0) return;
+    switch (deg) {
+        case -1: frame_project_kernel<-1><<<grid, 256, 0, st>>>(a); break;
+        case 0: frame_project_kernel<0><<<grid, 256, 0, st>>>(a); break;
+        case 1: frame_project_kernel<1><<<grid, 256, 0, st>>>(a); break;
+        case 2: frame_project_kernel<2><<<grid, 256, 0, st>>>(a); break;
+        default: frame_project_kernel<3><<<grid, 256, 0, st>>>(a); break;
+    }
+}
+
+void launch_count_stage(const FrameArgs& a, cudaStream_t st)
+{
+    const unsigned grid = (unsigned)a.num_tiles;
+    if (grid == 0) return;
+    count_stage_kernel<<<grid, 256, 0, st>>>(a);
+}
+
+void launch_emit(const EmitArgs& a, cudaStream_t st)
+{
+    const int64_t items = (int64_t)a.num_views * a.n;
+    const unsigned grid = (unsigned)((items + 255) / 256);
+    if (grid == 0) return;
+    emit_kernel<<<grid, 256, 0, st>>>(a);
+}
+
+}  // namespace gs

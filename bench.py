@@ -1,0 +1,297 @@
+"""Benchmark of the gs_b200 frame pipeline on the headline workload:
+3M Gaussians, SH degree 3, 64 views on an orbit ring at 1280x720 /
+1600x900 / 1920x1080, all rendered as one batched frame.  A step is one
+batched frame of the 64 views; the metric is views/s (whole job).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One process per GPU (torchrun for N > 1).  Views shard across ranks as
+independent replicas (each rank renders its own 64-view batch of the
+resident scene; there is no collective in the frame), so scaling is weak.
+--impl reference times the CPU rendition of the same pipeline (the oracle
+restatement of the reference's stages, OpenMP over the host cores) on a
+bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+VIEWS = 64
+N_GAUSS = 3_000_000
+RING_RADIUS = 15.0
+WORKLOAD = "3M Gaussians SH3, 64-view orbit ring r=15, 1280x720/1600x900/1920x1080 cycling, one batched frame"
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def make_workload(gs, rank=0):
+    sc = gs.scenes.config_scene("batch3m")
+    eyes = gs.scenes.orbit_ring(VIEWS, RING_RADIUS, seed=1000 + rank)
+    cams = []
+    for i, e in enumerate(eyes):
+        W, H = gs.scenes.BATCH_RESOLUTIONS[i % 3]
+        cams.append(gs.look_at(e, (0, 0, 0), (0, 1, 0), 50.0, W, H, 0.1, 100.0))
+    return sc, cams
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, index=0):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        self.p.wait()
+        self.f.flush()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        reasons = set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            for k, nm in enumerate(names):
+                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(gs, sc, cams, sample_views=1, threads=None):
+    """The oracle (CPU rendition of the five stages) over a bounded sample of views."""
+    import oracle
+    O = oracle.get()
+    if threads:
+        O.set_threads(threads)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    rc = gs.RenderConfig()
+    t0 = time.perf_counter()
+    for v in range(sample_views):
+        O.render(sc, sh, cams[v], rc)
+    dt = time.perf_counter() - t0
+    return {"value": sample_views / dt, "unit": "views/s", "cores": O.max_threads(), "kind": "port",
+            "sample": f"{sample_views} of the 64 views ({cams[0].GetWidth()}x{cams[0].GetHeight()}), full frame "
+                      f"(SH3 + project + build + sort + raster) of the 3M scene, {dt:.1f} s"}
+
+
+def run_reference(args, rank, world):
+    import torch.distributed as dist
+    if rank != 0:
+        return
+    gs = importlib.import_module("3dgaussianrenderer_b200")
+    sc, cams = make_workload(gs)
+    import oracle
+    O = oracle.get()
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    rc = gs.RenderConfig()
+    for w in range(args.warmup):
+        O.render(sc, sh, cams[w % VIEWS], rc)
+    times = []
+    for s in range(args.steps):
+        t0 = time.perf_counter()
+        O.render(sc, sh, cams[s % VIEWS], rc)
+        times.append(time.perf_counter() - t0)
+    tot = sum(times)
+    value = args.steps / tot
+    line = {
+        "impl": "reference", "metric": "views/s", "value": value, "unit": "views/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "step": "one view of the workload rendered on the host cores",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": "views/s", "cores": O.max_threads(), "kind": "port",
+                         "sample": "each step renders one of the 64 views (full frame, SH3) with the oracle "
+                                   "restatement of the reference stages, OpenMP"},
+        "e2e": {"value": value, "unit": "views/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    gs = importlib.import_module("3dgaussianrenderer_b200")
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    ctx = gs.Context(local_rank)
+    sc, cams = make_workload(gs, rank)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    rc = gs.RenderConfig()
+    outs = [torch.empty((c.GetHeight(), c.GetWidth(), 4), dtype=torch.uint8, device=dev) for c in cams]
+    stream = torch.cuda.current_stream(dev)
+
+    def step():
+        return gs.render_batch(ctx, scene, cams, rc, outs, stream)
+
+    for _ in range(args.warmup):
+        st = step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = Clocks(local_rank) if rank == 0 else None
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    stages = {"project_ms": 0.0, "build_tile_ms": 0.0, "sort_ms": 0.0, "raster_ms": 0.0}
+    launches = 0
+    keys = 0
+    e0.record(stream)
+    for _ in range(args.steps):
+        st = step()
+        for k in stages:
+            stages[k] += st[k]
+        launches += st["kernel_launches"]
+        keys = st["num_keys"]
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    clocks = clk.stop() if clk else None
+    t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * VIEWS * args.steps / (ms_max / 1e3)
+
+    # e2e through the public host-buffer API: camera upload + images back to pinned host memory
+    total_bytes = sum(c.GetWidth() * c.GetHeight() * 4 for c in cams)
+    host = torch.empty(total_bytes, dtype=torch.uint8).pin_memory()
+    host_np = host.numpy()
+    for _ in range(max(1, args.warmup // 2)):
+        gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
+    f1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = f0.elapsed_time(f1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * VIEWS * args.steps / (float(t.item()) / 1e3)
+
+    # plain single-view path over the same views (for the batched/plain ratio)
+    plain_views = min(VIEWS, 16)
+    for v in range(2):
+        gs.render(ctx, scene, cams[v], rc, outs[v], stream)
+    torch.cuda.synchronize()
+    g0 = torch.cuda.Event(enable_timing=True)
+    g1 = torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    for v in range(plain_views):
+        gs.render(ctx, scene, cams[v], rc, outs[v], stream)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    plain_value = plain_views / (g0.elapsed_time(g1) / 1e3)
+
+    if rank != 0:
+        return
+    hbm, peak_kind = peaks()
+    per = {k: v / args.steps for k, v in stages.items()}
+    K = keys
+    passes = (gs.key_bits(int(st["num_tiles"])) + 7) // 8
+    # algorithmic bytes per launch (HBM-bound stages)
+    n_items = N_GAUSS * VIEWS
+    alg = {
+        "project_ms": n_items * 32 + (N_GAUSS * 192 if True else 0) * VIEWS + n_items * 76,
+        "build_tile_ms": n_items * 8 + K * 12,
+        "sort_ms": K * (8 + 24 * passes),
+    }
+    ach = {k: alg[k] / (per[k] / 1e3) / 1e9 for k in alg if per[k] > 0}
+    dom = max(per, key=per.get)
+    dom_hbm = max(ach, key=lambda k: per[k])
+    roof = {"bound": "hbm", "kernel": dom_hbm.replace("_ms", ""), "achieved": ach[dom_hbm], "peak": hbm,
+            "unit": "GB/s", "frac": ach[dom_hbm] / hbm, "traffic": None,
+            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
+            "stage_ms": per, "stage_gbs": ach, "dominant_stage": dom}
+    cpu = cpu_baseline(gs, sc, cams, sample_views=1) if (world == 1 and not args.no_cpu) else None
+    line = {
+        "metric": "views/s", "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "views_per_step": VIEWS, "gaussians": N_GAUSS, "sh_degree": 3,
+                   "termination": "per-pixel T<1e-4", "tiles": "16x16", "keys_per_step": K,
+                   "l2": "inputs larger than L2 (scene 672 MB, per-view buffers ~15 GB)", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "views/s", "h2d_bytes_per_step": VIEWS * 200,
+                "d2h_bytes_per_step": total_bytes},
+        "plain_views_per_s": plain_value,
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        if args.impl == "ours":
+            torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl" if args.impl == "ours" else "gloo",
+                                timeout=datetime.timedelta(seconds=600))
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank, world)
+        else:
+            run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+            dist.barrier()
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

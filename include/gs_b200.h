@@ -1,0 +1,183 @@
+/*
+ * gs_b200 — B200-native 3D Gaussian splatting frame pipeline, C ABI.
+ *
+ * Drop-in for the stage API of RobinSongx/3DGaussianRenderer
+ * (core/gaussian_render.cuh:113-126, implemented in core/gaussian_render.cu)
+ * and the engine behind its Renderer API (core/renderer.h:13-50).  All
+ * entry points are extern "C", take plain pointers and sizes, return an
+ * int status (GS_OK = 0) and never exit the process.  Device pointers are
+ * marked d_; host pointers h_.  `stream` is a cudaStream_t passed as void*
+ * (NULL = legacy default stream).
+ *
+ * Buffer layouts are the reference's:
+ *   position          float4[n]  (x, y, z, opacity)                 main.cpp:295
+ *   scale_rotation    float4[n]  (sx, sy, sz, quat8 bit-cast)        ply_parser.cpp:385-388
+ *                     quat8: x<<24 | y<<16 | z<<8 | w, byte = (q+1)/2*255
+ *   sh                float[ceil(n/256)*256*sh_count] grouped as
+ *                     [group][coefficient][256], RGB interleaved per
+ *                     coefficient                                 main.cpp:147-177
+ *   color             float4[n]  (r, g, b, opacity)
+ *   xy / z            float2[n] / float[n]  clip-space centre / depth
+ *   ellipse           float4[n]  (cos, sin, extent.x, extent.y)
+ *   conic             float4[n]  (a, b, c, 0)
+ *   keys / values     uint64[K] (tile << 32 | quantised depth) / int32[K]
+ *   ranges            int32[2 * tiles]  [first, one-past-last)
+ *   rgba              uint8[4 * W * H], row 0 = bottom
+ */
+#ifndef GS_B200_H
+#define GS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define GS_API __attribute__((visibility("default")))
+#else
+#define GS_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    GS_OK = 0,
+    GS_ERR_INVALID = 1,        /* bad argument */
+    GS_ERR_OOM = 2,            /* device allocation failed */
+    GS_ERR_CAPACITY = 3,       /* a caller-sized buffer is too small */
+    GS_ERR_DEVICE_TIMEOUT = 4, /* a bounded device wait gave up */
+    GS_ERR_CUDA = 5,           /* other CUDA error (see gs_last_error_string) */
+    GS_ERR_NO_DEVICE = 6       /* no usable sm_100 device */
+};
+
+enum { GS_TERM_REFERENCE = 0, GS_TERM_TMIN = 1 };
+
+/* Per-view camera.  Same fields as the reference's CameraData
+ * (gaussian_render.cuh:16-25) minus the unused projection matrices, plus
+ * the image size. */
+typedef struct gs_camera {
+    float view[16];            /* world -> view, column-major */
+    float position[3];         /* camera centre, world space */
+    float fov_cotangent[2];    /* (cot(fovy/2)/aspect, cot(fovy/2))   main.cpp:352-354 */
+    float depth_scale_bias[2]; /* (-2/(f-n), -(f+n)/(f-n))            main.cpp:355-358 */
+    float aspect;
+    int32_t width, height;
+} gs_camera;
+
+/* Pipeline options. */
+typedef struct gs_render_cfg {
+    int32_t sh_max_degree; /* SH degrees evaluated: 2 = reference (gaussian_render.cu:62-91), 3 = full */
+    int32_t termination;   /* GS_TERM_REFERENCE (T<=0.02 tile-wide every 32 entries) or GS_TERM_TMIN */
+    float t_min;           /* per-pixel transmittance floor for GS_TERM_TMIN (1e-4) */
+    int32_t tile_w, tile_h;/* 16x16 (reference), 16x8 or 8x8 */
+    int32_t raster_batch;  /* splats staged per shared-memory batch: 32..256 (0 = default) */
+} gs_render_cfg;
+
+/* Per-stage device times of one frame, same fields as the reference's
+ * RenderStats (core/types.h:26-33), plus the tile-list size. */
+typedef struct gs_stats {
+    double sh_eval_ms, project_ms, build_tile_ms, sort_ms, raster_ms, total_ms;
+    int64_t num_keys;
+    int64_t num_tiles;
+    int64_t kernel_launches; /* gs_b200 kernels launched for the frame */
+} gs_stats;
+
+typedef struct gs_ctx gs_ctx;
+typedef struct gs_scene gs_scene;
+
+/* ---- library / context ------------------------------------------------ */
+
+GS_API int gs_version(void);
+GS_API const char* gs_status_string(int status);
+GS_API const char* gs_last_error_string(void);
+GS_API void gs_default_cfg(gs_render_cfg* cfg);
+/* Fills a gs_camera from a look-at pose, following camera.cpp:30-55 with the
+ * built frame loop's depth convention (main.cpp:352-358). */
+GS_API void gs_camera_look_at(gs_camera* cam, const float eye[3], const float target[3], const float up[3],
+                       float fovy_rad, int32_t width, int32_t height, float znear, float zfar);
+
+GS_API int gs_ctx_create(int device, gs_ctx** out);
+GS_API int gs_ctx_destroy(gs_ctx* ctx);
+/* Device bytes currently held by the context's frame buffers. */
+GS_API int64_t gs_ctx_device_bytes(const gs_ctx* ctx);
+
+/* ---- scenes (Renderer::UploadModel, core/renderer.cpp:36-88) ---------- */
+
+/* Uploads host arrays (reference layouts above) into a device-resident,
+ * immutable scene.  h_color may be NULL when sh_degree > 0; h_sh may be NULL
+ * when sh_degree == 0.  sh_count = 3 * (sh_degree + 1)^2. */
+GS_API int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
+                    const float* h_color, const float* h_sh, int32_t sh_degree, gs_scene** out);
+GS_API int gs_scene_destroy(gs_scene* scene);
+GS_API int64_t gs_scene_size(const gs_scene* scene);
+GS_API int64_t gs_scene_device_bytes(const gs_scene* scene);
+
+/* ---- whole frame (Renderer::Render, core/renderer.cpp:94-139) ---------- */
+
+/* Renders one view into d_rgba (device, 4*W*H bytes, cleared by the call).
+ * Stats may be NULL.  The call returns after the frame completed. */
+GS_API int gs_render(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cam, const gs_render_cfg* cfg, uint8_t* d_rgba,
+              gs_stats* stats, void* stream);
+
+/* Same, with the image returned into host memory h_rgba (pinned or not). */
+GS_API int gs_render_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cam, const gs_render_cfg* cfg,
+                   uint8_t* h_rgba, gs_stats* stats, void* stream);
+
+/* Renders V views (any mix of sizes) of one scene in one batched frame:
+ * one flattened tile space with the view in the key's high bits, one
+ * persistent rasteriser, replayed as a CUDA graph when the same view set
+ * shape is rendered again.  d_rgba[v] (device) receive 4*W_v*H_v bytes. */
+GS_API int gs_render_batch(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                    const gs_render_cfg* cfg, uint8_t* const* d_rgba, gs_stats* stats, void* stream);
+/* Same, images copied into one host buffer: view v at byte offset
+ * sum_{u<v} 4*W_u*H_u. */
+GS_API int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                         const gs_render_cfg* cfg, uint8_t* h_rgba, gs_stats* stats, void* stream);
+
+/* ---- stage API (core/gaussian_render.cuh:113-126) ---------------------- */
+/* Explicit-argument replacements of the reference's constant-memory stage
+ * functions.  All pointers are device pointers; every call is asynchronous
+ * on `stream` unless stated otherwise. */
+
+/* evaluateSphericalHarmonics (gaussian_render.cu:96-133) */
+GS_API int gs_stage_sh(int64_t n, const float* d_position, const float* d_sh, int32_t sh_count, int32_t eval_degree,
+                const gs_camera* cam, float* d_color, void* stream);
+
+/* evaluateSplatClipData (gaussian_render.cu:135-232) */
+GS_API int gs_stage_project(int64_t n, const float* d_position, const float* d_scale_rotation, const gs_camera* cam,
+                     float* d_xy, float* d_z, float* d_ellipse, float* d_conic, void* stream);
+
+/* buildTileList (gaussian_render.cu:312-589).  Exact: counts every
+ * Gaussian's overlapping tiles, scans, and emits keys in Gaussian order.
+ * Synchronises once to read K into *out_num_keys.  Returns
+ * GS_ERR_CAPACITY (and writes nothing) when K > capacity. */
+GS_API int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, const float* d_ellipse,
+                   const gs_camera* cam, const gs_render_cfg* cfg, uint64_t* d_keys, int32_t* d_values,
+                   int64_t capacity, int64_t* out_num_keys, void* stream);
+
+/* sortTileList (gaussian_render.cu:591-632): stable LSD radix sort of K
+ * pairs on key bits [0, key_bits), onesweep with decoupled look-back.  The
+ * result ends in (d_keys, d_values) when *out_selector == 0 and in
+ * (d_keys_alt, d_values_alt) when 1.  Scratch comes from the context. */
+GS_API int gs_stage_sort(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, uint64_t* d_keys, int32_t* d_values,
+                  uint64_t* d_keys_alt, int32_t* d_values_alt, int32_t* out_selector, void* stream);
+
+/* evaluateTileRange (gaussian_render.cu:634-677).  Fills all 2*num_tiles
+ * entries: tiles without keys get (-1, -1) as after the reference's
+ * 0xFF clear (main.cpp:365). */
+GS_API int gs_stage_ranges(int64_t num_keys, const uint64_t* d_keys, int64_t num_tiles, int32_t* d_ranges, void* stream);
+
+/* rasterizeTile (gaussian_render.cu:679-775).  d_rgba must be cleared by
+ * the caller (tiles without splats are not written, main.cpp:363). */
+GS_API int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_t* d_ranges, const int32_t* d_values,
+                    const float* d_xy, const float* d_conic, const float* d_color, uint8_t* d_rgba, void* stream);
+
+/* Number of tiles of a W x H image with the cfg's tile shape. */
+GS_API int64_t gs_num_tiles(int32_t width, int32_t height, const gs_render_cfg* cfg);
+/* Significant key bits for `num_tiles` tiles: 32 + ceil(log2(num_tiles)). */
+GS_API int32_t gs_key_bits(int64_t num_tiles);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,286 @@
+// Reference harness: a C-ABI around the reference's own CUDA stage API
+// (core/gaussian_render.cuh:113-126), compiled from the reference sources
+// into oracle/_ref/libgsref.so by oracle/ref/build_ref.sh.
+//
+// TEST INFRASTRUCTURE ONLY.  Nothing in the product links or calls this
+// library; tests/, the golden-fixture generator and bench.py's reference
+// timing load it to obtain the reference's outputs and frame times on the
+// same B200 and the same inputs.
+//
+// It reproduces the headless part of the reference frame loop
+// (app/main.cpp:360-432): clear the colour buffer and tile ranges, upload
+// GlobalArgs/TileListArgs to constant memory, then SH -> project -> build ->
+// sort -> ranges -> raster, each stage wrapped in the reference's blocking
+// CudaTimer.  The probe kernels at the end call the reference's device
+// helpers (core/gaussian_render.cu:234-310) on caller-supplied inputs so the
+// CPU oracle's float semantics can be pinned against them.
+
+#include "gaussian_render.cu"  // patched copy produced by build_ref.sh
+
+#include <cstring>
+
+static_assert(sizeof(CameraData) == 56 * sizeof(float), "CameraData layout");
+
+namespace
+{
+GlobalArgs g_HostArgs;
+TileListArgs g_HostTileArgs;
+void* g_SortTemp = nullptr;
+size_t g_SortTempBytes = 0;
+CudaTimer* g_Timer = nullptr;
+
+CudaTimer& timer()
+{
+    if (!g_Timer)
+    {
+        g_Timer = new CudaTimer();
+    }
+    return *g_Timer;
+}
+}  // namespace
+
+extern "C" {
+
+// camera56: viewProjection[16], projection[16], view[16] (glm column-major),
+// fovCotangent[2], depthScaleBias[2], position[3], aspect.
+int gsref_set_global_args(const float* camera56,
+                          void* position,
+                          void* scaleAndRotation,
+                          void* color,
+                          int shDegree,
+                          int shCount,
+                          void* sh,
+                          void* xy,
+                          void* z,
+                          void* conic,
+                          void* ellipse,
+                          int splatCount,
+                          void* backBuffer,
+                          void* tileRange)
+{
+    std::memset(&g_HostArgs, 0, sizeof(g_HostArgs));
+    std::memcpy(&g_HostArgs.cameraData, camera56, sizeof(CameraData));
+    g_HostArgs.position = (float4*) position;
+    g_HostArgs.scaleAndRotation = (float4*) scaleAndRotation;
+    g_HostArgs.color = (float4*) color;
+    g_HostArgs.sphericalHarmonicsDegree = shDegree;
+    g_HostArgs.sphericalHarmonicsCount = shCount;
+    g_HostArgs.sphericalHarmonics = (float*) sh;
+    g_HostArgs.positionClipSpaceXY = (float2*) xy;
+    g_HostArgs.positionClipSpaceZ = (float*) z;
+    g_HostArgs.conic = (float4*) conic;
+    g_HostArgs.screenEllipse = (float4*) ellipse;
+    g_HostArgs.splatCount = splatCount;
+    g_HostArgs.backBuffer = (uchar4*) backBuffer;
+    g_HostArgs.tileRange = (int32_t*) tileRange;
+    setGlobalArgs(&g_HostArgs);
+    return (int) cudaGetLastError();
+}
+
+int gsref_set_tile_list_args(void* keys, void* values, int size, int capacity)
+{
+    g_HostTileArgs.keys = (uint64_t*) keys;
+    g_HostTileArgs.values = (int32_t*) values;
+    g_HostTileArgs.size = size;
+    g_HostTileArgs.capacity = capacity;
+    setTileListArgs(&g_HostTileArgs);
+    return (int) cudaGetLastError();
+}
+
+float gsref_eval_sh(int n)
+{
+    evaluateSphericalHarmonics(timer(), n);
+    return timer().getElapseTimedMs();
+}
+
+float gsref_eval_clip(int n)
+{
+    evaluateSplatClipData(timer(), n);
+    return timer().getElapseTimedMs();
+}
+
+int gsref_build(int numBlocks, int capacity, float* ms)
+{
+    int k = buildTileList(timer(), numBlocks, capacity);
+    if (ms)
+    {
+        *ms = timer().getElapseTimedMs();
+    }
+    return k;
+}
+
+// Sorts with the reference's sortTileList (CUB DeviceRadixSort over bits
+// [0,44)).  *selector receives 0 when the result is in keys0/vals0 and 1
+// when it is in keys1/vals1.
+float gsref_sort(int size, void* keys0, void* keys1, void* vals0, void* vals1, int* selector)
+{
+    DoubleBuffer<uint64_t> k((uint64_t*) keys0, (uint64_t*) keys1);
+    DoubleBuffer<int32_t> v((int32_t*) vals0, (int32_t*) vals1);
+    sortTileList(timer(), size, g_SortTemp, g_SortTempBytes, k, v);
+    *selector = (k.current() == (uint64_t*) keys0) ? 0 : 1;
+    return timer().getElapseTimedMs();
+}
+
+float gsref_ranges(int size)
+{
+    evaluateTileRange(timer(), size);
+    return timer().getElapseTimedMs();
+}
+
+float gsref_raster()
+{
+    rasterizeTile(timer());
+    return timer().getElapseTimedMs();
+}
+
+// One headless frame in the order of app/main.cpp:360-432.  Buffers are
+// owned by the caller; keys*/vals* hold `capacity` entries each.
+// stageMs[6] = sh, clip, build, sort, ranges, raster (reference timers, each
+// including the blocking sync of CudaTimer::stop).  Returns the tile-list
+// size K (== capacity when the list saturated, as in the reference).
+int gsref_render_frame(const float* camera56,
+                       void* position,
+                       void* scaleAndRotation,
+                       void* color,
+                       int shDegree,
+                       int shCount,
+                       void* sh,
+                       void* xy,
+                       void* z,
+                       void* conic,
+                       void* ellipse,
+                       int splatCount,
+                       void* backBuffer,
+                       void* tileRange,
+                       void* keys0,
+                       void* keys1,
+                       void* vals0,
+                       void* vals1,
+                       int capacity,
+                       int buildBlocks,
+                       float* stageMs,
+                       float* frameMs,
+                       int* selector)
+{
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0);
+
+    cudaMemset(backBuffer, 0, sizeof(uchar4) * k_ScreenSize * k_ScreenSize);
+    cudaMemset(tileRange, 0xFF, sizeof(int32_t) * k_TotalTiles * 2);
+    gsref_set_global_args(camera56, position, scaleAndRotation, color, shDegree, shCount, sh, xy, z, conic,
+                          ellipse, splatCount, backBuffer, tileRange);
+    gsref_set_tile_list_args(keys0, vals0, 0, capacity);
+
+    for (int i = 0; i < 6; ++i)
+    {
+        stageMs[i] = 0.0f;
+    }
+    if (shDegree != 0)
+    {
+        stageMs[0] = gsref_eval_sh(splatCount);
+    }
+    stageMs[1] = gsref_eval_clip(splatCount);
+    int size = gsref_build(buildBlocks, capacity, &stageMs[2]);
+    gsref_set_tile_list_args(keys0, vals0, size, capacity);
+    stageMs[3] = gsref_sort(size, keys0, keys1, vals0, vals1, selector);
+    void* kc = (*selector == 0) ? keys0 : keys1;
+    void* vc = (*selector == 0) ? vals0 : vals1;
+    gsref_set_tile_list_args(kc, vc, size, capacity);
+    if (size != 0)
+    {
+        stageMs[4] = gsref_ranges(size);
+    }
+    stageMs[5] = gsref_raster();
+    cudaDeviceSynchronize();
+
+    cudaEventRecord(e1);
+    cudaEventSynchronize(e1);
+    cudaEventElapsedTime(frameMs, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return size;
+}
+
+int gsref_sync()
+{
+    return (int) cudaDeviceSynchronize();
+}
+
+int gsref_screen_size()
+{
+    return k_ScreenSize;
+}
+
+int gsref_tile_size()
+{
+    return k_TileSize;
+}
+
+// ---- probes of the reference's device helpers ------------------------------
+
+// ell: n x 6 floats (centre.x, centre.y, cos, sin, extent.x, extent.y)
+// rect: n x 4 floats (min.x, min.y, max.x, max.y)
+__global__ void gsrefProbeOverlapKernel(int n, const float* ell, const float* rect, int* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        Ellipse e;
+        e.center = glm::vec2(ell[6 * i + 0], ell[6 * i + 1]);
+        e.cosSin = glm::vec2(ell[6 * i + 2], ell[6 * i + 3]);
+        e.extent = glm::vec2(ell[6 * i + 4], ell[6 * i + 5]);
+        Rect r;
+        r.min = glm::vec2(rect[4 * i + 0], rect[4 * i + 1]);
+        r.max = glm::vec2(rect[4 * i + 2], rect[4 * i + 3]);
+        out[i] = ellipseRectOverlap(e, r) ? 1 : 0;
+    }
+}
+
+__global__ void gsrefProbeAabbKernel(int n, const float* ell, float* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        Ellipse e;
+        e.center = glm::vec2(ell[6 * i + 0], ell[6 * i + 1]);
+        e.cosSin = glm::vec2(ell[6 * i + 2], ell[6 * i + 3]);
+        e.extent = glm::vec2(ell[6 * i + 4], ell[6 * i + 5]);
+        Rect r = getAABBRect(e);
+        out[4 * i + 0] = r.min.x;
+        out[4 * i + 1] = r.min.y;
+        out[4 * i + 2] = r.max.x;
+        out[4 * i + 3] = r.max.y;
+    }
+}
+
+__global__ void gsrefProbeKeyKernel(int n, const int* tile, const float* depth, unsigned long long* out)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+    {
+        out[i] = getKey(tile[i], depth[i]);
+    }
+}
+
+int gsref_probe_overlap(int n, const void* ell, const void* rect, void* out)
+{
+    gsrefProbeOverlapKernel<<<(n + 255) / 256, 256>>>(n, (const float*) ell, (const float*) rect, (int*) out);
+    return (int) cudaDeviceSynchronize();
+}
+
+int gsref_probe_aabb(int n, const void* ell, void* out)
+{
+    gsrefProbeAabbKernel<<<(n + 255) / 256, 256>>>(n, (const float*) ell, (float*) out);
+    return (int) cudaDeviceSynchronize();
+}
+
+int gsref_probe_key(int n, const void* tile, const void* depth, void* out)
+{
+    gsrefProbeKeyKernel<<<(n + 255) / 256, 256>>>(n, (const int*) tile, (const float*) depth,
+                                                   (unsigned long long*) out);
+    return (int) cudaDeviceSynchronize();
+}
+
+}  // extern "C"

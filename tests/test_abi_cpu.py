@@ -1,0 +1,67 @@
+"""CPU checks of the C ABI: the library loads, exports every entry point
+include/gs_b200.h declares, and reports errors without a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import ROOT
+
+HEADER = os.path.join(ROOT, "include", "gs_b200.h")
+
+
+def declared_symbols():
+    text = open(HEADER).read()
+    return sorted(set(re.findall(r"^GS_API\s+[\w\s\*]+?\b(gs_\w+)\s*\(", text, flags=re.M)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    for s in ("gs_render", "gs_stage_sh", "gs_stage_project", "gs_stage_build", "gs_stage_sort", "gs_stage_ranges",
+              "gs_stage_raster", "gs_render_batch", "gs_scene_create"):
+        assert s in syms
+
+
+def test_library_exports_every_declared_symbol(gs):
+    lib = ctypes.CDLL(gs.LIB_PATH)
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_status_strings_and_helpers(gs):
+    assert gs.lib.gs_version() >= 100
+    for code in range(0, 7):
+        assert gs.lib.gs_status_string(code)
+    rc = gs.RenderConfig()
+    assert gs.num_tiles(1920, 1080, rc) == 120 * 68
+    assert gs.num_tiles(1024, 1024, gs.RenderConfig.reference()) == 4096
+    assert gs.key_bits(4096) == 44
+    assert gs.key_bits(8160) == 45
+    assert gs.key_bits(1) == 32
+
+
+def test_camera_matches_reference_conventions(gs):
+    cam = gs.look_at((0, 0, 3), (0, 0, 0), (0, 1, 0), 60.0, 800, 600, 0.1, 100.0)
+    c = cam.c
+    coty = 1 / np.tan(np.radians(30))
+    assert np.isclose(c.fov_cotangent[1], coty, rtol=1e-6)
+    assert np.isclose(c.fov_cotangent[0], coty / (800 / 600), rtol=1e-6)
+    assert np.isclose(c.depth_scale_bias[0], -2 / 99.9, rtol=1e-6)
+    assert np.isclose(c.depth_scale_bias[1], -100.1 / 99.9, rtol=1e-6)
+    V = np.array(c.view, np.float32).reshape(4, 4)  # [col][row]
+    # the origin lies 3 units in front (view z = -3)
+    p = V.T @ np.array([0, 0, 0, 1], np.float32)
+    assert np.allclose(p[:3], [0, 0, -3], atol=1e-6)
+
+
+@pytest.mark.skipif(os.environ.get("CUDA_VISIBLE_DEVICES", None) is None and __import__("torch").cuda.is_available(),
+                    reason="a GPU is present")
+def test_errors_without_gpu(gs):
+    h = ctypes.c_void_p()
+    st = gs.lib.gs_ctx_create(0, ctypes.byref(h))
+    assert st in (gs.GS_ERR_NO_DEVICE, gs.GS_ERR_CUDA)
+    # null arguments are rejected before any device work
+    assert gs.lib.gs_render(None, None, None, None, None, None, None) == gs.GS_ERR_INVALID
+    assert gs.lib.gs_stage_ranges(-1, None, 0, None, None) == gs.GS_ERR_INVALID
