@@ -172,6 +172,24 @@ GS_API int gs_stage_ranges(int64_t num_keys, const uint64_t* d_keys, int64_t num
 GS_API int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_t* d_ranges, const int32_t* d_values,
                     const float* d_xy, const float* d_conic, const float* d_color, uint8_t* d_rgba, void* stream);
 
+/* ---- model ingest (parsePly / savePly, core/ply_parser.cpp:15-393) ------ */
+/* Binary little-endian PLY with float properties named as the INRIA 3DGS
+ * exporter writes them (x y z rot_0..3 scale_0..2 f_dc_0..2 f_rest_* opacity).
+ * Errors are GS_ERR_INVALID with the reason in gs_ply_last_error(). */
+GS_API int gs_ply_info(const char* path, int64_t* out_n, int32_t* out_sh_degree);
+GS_API const char* gs_ply_last_error(void);
+/* Applies the reference's load transforms (normalised quaternion -> 8-bit
+ * encoding, exp(scale), sigmoid(opacity), DC*C0+0.5) and writes the host
+ * buffers in the layouts above; h_sh_grouped (SH scenes) takes
+ * ceil(n/256)*256*sh_count floats.  Any output may be NULL; bounds[6] =
+ * (min xyz, max xyz) as the reference computes them. */
+GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotation, float* h_color,
+                       float* h_sh_grouped, float* bounds);
+/* Writes a scene as a PLY that gs_ply_read (and the reference's parsePly)
+ * reads back; SH scenes get f_rest_* (channel-major). */
+GS_API int gs_ply_write(const char* path, int64_t n, const float* h_position, const float* h_scale_rotation,
+                        const float* h_color, const float* h_sh_grouped, int32_t sh_degree);
+
 /* Number of tiles of a W x H image with the cfg's tile shape. */
 GS_API int64_t gs_num_tiles(int32_t width, int32_t height, const gs_render_cfg* cfg);
 /* Significant key bits for `num_tiles` tiles: 32 + ceil(log2(num_tiles)). */

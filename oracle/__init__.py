@@ -74,6 +74,7 @@ class Oracle:
         sig = {
             "gso_set_fma_mode": (None, [ctypes.c_int]),
             "gso_get_fma_mode": (ctypes.c_int, []),
+            "gso_set_u8_mode": (None, [ctypes.c_int]),
             "gso_set_threads": (None, [ctypes.c_int]),
             "gso_max_threads": (ctypes.c_int, []),
             "gso_sh": (None, [_I64, _P, _P, _I32, _I32, _P, _P]),
@@ -95,6 +96,9 @@ class Oracle:
 
     def set_fma_mode(self, m: int):
         self.lib.gso_set_fma_mode(m)
+
+    def set_u8_mode(self, m: int):
+        self.lib.gso_set_u8_mode(m)
 
     def fma_mode(self) -> int:
         return self.lib.gso_get_fma_mode()

@@ -87,10 +87,17 @@ static inline uint32_t cvt_u32(float x)
     if (x >= 4294967296.0f) return 0xFFFFFFFFu;
     return (uint32_t)x;
 }
-/* float -> unsigned char as the reference's uchar4 store (gaussian_render.cu:752-754):
- * truncate and saturate to [0,255], NaN -> 0. */
+/* float -> unsigned char as the reference's uchar4 store (gaussian_render.cu:752-754).
+ * Mode 0: truncate and saturate to [0,255]; 1: truncate to int32 (saturating), keep
+ * the low byte; 2: truncate to uint32 (negatives -> 0, saturating), keep the low byte.
+ * The reference's kernels do 2 (pinned by the out-of-range-colour golden frame):
+ * a colour of 256/255 stores 0, not 255. */
+static int g_u8 = 2;
+void gso_set_u8_mode(int mode) { g_u8 = mode; }
 static inline uint8_t cvt_u8(float x)
 {
+    if (g_u8 == 1) return (uint8_t)((uint32_t)cvt_s32(x) & 0xFFu);
+    if (g_u8 == 2) return (uint8_t)(cvt_u32(x) & 0xFFu);
     if (x != x || x <= 0.0f) return 0;
     if (x >= 255.0f) return 255;
     return (uint8_t)x;
@@ -419,8 +426,10 @@ static rect_t aabb_rect(const ellipse_t* e)
         int bb = j & 1, tb = j >> 1;
         float sr = (float)(bb ^ tb) * 2.0f - 1.0f;
         float su = (float)tb * 2.0f - 1.0f;
-        float vx = rx * sr + ux * su;
-        float vy = ry * sr + uy * su;
+        /* right*r + up*u: nvcc keeps the principal-axis product unrounded,
+         * fma(cos*r, extent.x, round(sin*extent.y)*u) (pinned by the probes) */
+        float vx = g_fma ? fmaf(e->cs * sr, e->ex, ux * su) : rx * sr + ux * su;
+        float vy = g_fma ? fmaf(e->sn * sr, e->ex, uy * su) : ry * sr + uy * su;
         r.x0 = gmin(r.x0, vx);
         r.y0 = gmin(r.y0, vy);
         r.x1 = gmax(r.x1, vx);

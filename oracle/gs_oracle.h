@@ -50,6 +50,9 @@ typedef struct gso_cfg {
 
 /* 0: no contraction; 1: fuse the first product of a sum; 2: fuse the last. */
 void gso_set_fma_mode(int mode);
+/* float -> uint8 conversion of the final colour: 0 saturate, 1 int32 low byte,
+ * 2 uint32 low byte (see gs_oracle.c). */
+void gso_set_u8_mode(int mode);
 int gso_get_fma_mode(void);
 void gso_set_threads(int n);
 int gso_max_threads(void);

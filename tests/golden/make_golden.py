@@ -110,10 +110,29 @@ def run_ref_frame(ref: oracle.Ref, scene: dict, cam) -> dict:
     kk = (k1 if sel.value else k0)[:size].cpu().numpy().view(np.uint64)
     vv = (v1 if sel.value else v0)[:size].cpu().numpy()
     kk, vv = canonical(kk, vv)
+    image_raw = img.cpu().numpy()
+    # The reference's emission order decides how entries with equal keys are
+    # blended, so its image is one sample of several.  Re-run its ranges and
+    # raster kernels on the canonical order (equal keys by index) to get the
+    # deterministic image of the same kernels.
+    ck = torch.from_numpy(kk.view(np.int64).copy()).to(dev)
+    cv = torch.from_numpy(vv.copy()).to(dev)
+    img.zero_()
+    ranges_c = torch.full((2 * 4096,), -1, dtype=torch.int32, device=dev)
+    ref.lib.gsref_set_global_args(cam56.ctypes.data, pos.data_ptr(), sr.data_ptr(), color.data_ptr(), deg, sh_count,
+                                  sh.data_ptr(), xy.data_ptr(), z.data_ptr(), conic.data_ptr(), ell.data_ptr(), n,
+                                  img.data_ptr(), ranges_c.data_ptr())
+    ref.lib.gsref_set_tile_list_args(ck.data_ptr(), cv.data_ptr(), size, cap)
+    if size:
+        ref.lib.gsref_ranges(size)
+    ref.lib.gsref_raster()
+    torch.cuda.synchronize()
+    assert np.array_equal(ranges_c.cpu().numpy(), ranges.cpu().numpy())
     out = {
+        "image_canonical": img.cpu().numpy(),
         "K": np.int64(size),
         "xy": xy.cpu().numpy(), "z": z.cpu().numpy(), "ell": ell.cpu().numpy(), "conic": conic.cpu().numpy(),
-        "keys": kk, "vals": vv, "ranges": ranges.cpu().numpy(), "image": img.cpu().numpy(),
+        "keys": kk, "vals": vv, "ranges": ranges.cpu().numpy(), "image": image_raw,
     }
     if deg > 0:
         out["color"] = color.cpu().numpy()

@@ -13,7 +13,8 @@ import numpy as np
 import pytest
 
 from conftest import golden_frames
-from helpers import camera_from_fixture, canonical, load_frame, psnr, bits_equal, scene_from_fixture
+from helpers import (camera_from_fixture, canonical, load_frame, psnr, bits_equal, scene_from_fixture,
+                     reference_image_check)
 
 torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
@@ -127,11 +128,10 @@ def test_raster_vs_reference(gs, name):
     gs.stage_raster(cam, rc, dev(d["ref_ranges"]), dev(d["ref_vals"]), dev(d["ref_xy"]), dev(d["ref_conic"]),
                     dev(color), img)
     out = img.cpu().numpy()
-    ref = d["ref_image"]
-    diff = np.abs(out.astype(int) - ref.astype(int))
-    assert diff.max() <= IMG_TOL
-    assert psnr(out, ref) >= PSNR_MIN
-    print(name, "raster identical pixels", float((diff.max(-1) == 0).mean()))
+    max_diff, p = reference_image_check(out, d)
+    assert max_diff <= IMG_TOL
+    assert p >= PSNR_MIN
+    print(name, "raster max diff", max_diff, "psnr", p)
 
 
 @pytest.mark.parametrize("name", golden_frames())
@@ -142,11 +142,10 @@ def test_full_frame_vs_reference(gs, ctx, name):
     sh = gs.scenes.grouped_sh(sc["sh"]) if sc["sh"] is not None else None
     scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, sc["sh_degree"], sc["color4"])
     img, st = gs.render_host(ctx, scene, cam, gs.RenderConfig.reference())
-    ref = d["ref_image"]
-    diff = np.abs(img.astype(int) - ref.astype(int))
     assert st["num_keys"] == int(d["ref_K"])
-    assert diff.max() <= IMG_TOL
-    assert psnr(img, ref) >= PSNR_MIN
+    max_diff, p = reference_image_check(img, d)
+    assert max_diff <= IMG_TOL
+    assert p >= PSNR_MIN
 
 
 # ---- against the CPU oracle at configuration sizes -------------------------------

@@ -7,7 +7,7 @@ import os
 import numpy as np
 import pytest
 
-from helpers import GOLDEN, camera_from_fixture, canonical, load_frame, psnr, bits_equal
+from helpers import GOLDEN, camera_from_fixture, canonical, load_frame, psnr, bits_equal, reference_image_check
 from conftest import golden_frames
 
 PROBES = os.path.join(GOLDEN, "probes.npz")
@@ -66,10 +66,9 @@ def test_oracle_raster_vs_reference(O, name):
     rc = gs.RenderConfig.reference()
     color = d["ref_color"] if "ref_color" in d else d["color4"]
     img = O.raster(cam, rc, d["ref_ranges"], d["ref_vals"], d["ref_xy"], d["ref_conic"], color)
-    ref = d["ref_image"]
-    diff = np.abs(img.astype(int) - ref.astype(int))
-    assert diff.max() <= 2, f"max abs diff {diff.max()}"
-    assert psnr(img, ref) >= 50.0
+    max_diff, p = reference_image_check(img, d)
+    assert max_diff <= 2, f"max abs diff {max_diff}"
+    assert p >= 50.0
 
 
 @pytest.mark.parametrize("name", golden_frames())
