@@ -107,7 +107,8 @@ struct gs_ctx {
     uint32_t epoch_scan = 1, epoch_sort = 1;
     DevBuf views;                          // ViewParams[]
     DevBuf color, xy, z, ell, conic, rect, offsets;  // per (view, Gaussian)
-    DevBuf scan_status;                    // frame kernel look-back words
+    DevBuf scan_status;                    // frame kernel look-back words, [view][group]
+    DevBuf view_stats;                     // int64 [2][views]: keys per view, first key of view
     DevBuf keys0, vals0, keys1, vals1;     // tile lists
     DevBuf sort_hist, sort_status;
     DevBuf ranges;
@@ -238,20 +239,26 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     const int64_t items = n * num_views;
     if (items >= (1ll << 31)) return fail(GS_ERR_INVALID, "views x Gaussians exceeds 2^31");
     const int64_t groups = (n + 255) / 256;
-    const int64_t blocks = groups * num_views;
+    // views per block: the SH chunk of a group is read once per block
+    const int vpb = std::min(num_views, 8);
+    const int64_t blocks = groups * ((num_views + vpb - 1) / vpb);
+    const int64_t chains = groups * num_views;
 
     // per-(view, Gaussian) buffers
     if (items > ctx->per_view_capacity) {
         const size_t m = (size_t)items;
         if (ctx->color.ensure(16 * m) || ctx->xy.ensure(8 * m) || ctx->z.ensure(4 * m) || ctx->ell.ensure(16 * m) ||
-            ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(8 * m))
+            ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(4 * m))
             return fail(GS_ERR_OOM, "splat buffers");
         ctx->per_view_capacity = items;
     }
-    if (sizeof(uint64_t) * (size_t)std::max<int64_t>(blocks, 1) > ctx->scan_status.bytes) {
-        if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(blocks, 1), true))
+    if (sizeof(uint64_t) * (size_t)std::max<int64_t>(chains, 1) > ctx->scan_status.bytes) {
+        if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)std::max<int64_t>(chains, 1), true))
             return fail(GS_ERR_OOM, "scan status");
     }
+    if (ctx->view_stats.ensure(sizeof(int64_t) * 2 * (size_t)num_views)) return fail(GS_ERR_OOM, "view stats");
+    int64_t* view_total = ctx->view_stats.as<int64_t>();
+    int64_t* view_base = view_total + num_views;
     if (ctx->ranges.ensure(sizeof(int32_t) * 2 * (size_t)tiles_total)) return fail(GS_ERR_OOM, "ranges");
 
     Counters* dc = ctx->counters.as<Counters>();
@@ -262,7 +269,9 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     // 1. SH + projection + exact tile counts + key offsets
     FrameArgs fa;
     fa.n = n;
+    fa.groups = groups;
     fa.num_views = num_views;
+    fa.views_per_block = vpb;
     fa.epoch = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
     fa.num_tiles = blocks;
     fa.pos = scene->pos.as<float4>();
@@ -277,16 +286,19 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     fa.ell = ctx->ell.as<float4>();
     fa.conic = ctx->conic.as<float4>();
     fa.rect = ctx->rect.as<int2>();
-    fa.offsets = ctx->offsets.as<int64_t>();
+    fa.offsets = ctx->offsets.as<int32_t>();
     fa.status = ctx->scan_status.as<uint64_t>();
     fa.tile_counter = &dc->frame_tile;
-    fa.total = &dc->total;
+    fa.view_total = view_total;
     fa.err = &dc->err;
     // degree-0 scenes blend the model colours (ply_parser.cpp:383,389); SH
     // scenes evaluate min(scene degree, cfg degree) (gaussian_render.cu:392)
     if (scene->sh_degree == 0 && !scene->color.p) return fail(GS_ERR_INVALID, "scene has no colour");
     const int deg = scene->sh_degree > 0 ? eval_degree(scene, cfg) : -1;
-    if (n > 0) launch_frame_project(fa, deg, st);
+    if (n > 0) {
+        launch_frame_project(fa, deg, st);
+        launch_view_base(view_total, num_views, view_base, &dc->total, st);
+    }
     GS_CUDA(cudaGetLastError());
     GS_CUDA(cudaEventRecord(ctx->ev[1], st));
     GS_CUDA(cudaMemcpyAsync(ctx->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -309,8 +321,9 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     ea.n = n;
     ea.num_views = num_views;
     ea.views = ctx->views.as<ViewParams>();
-    ea.offsets = ctx->offsets.as<int64_t>();
-    ea.total = &dc->total;
+    ea.offsets = ctx->offsets.as<int32_t>();
+    ea.view_total = view_total;
+    ea.view_base = view_base;
     ea.rect = ctx->rect.as<int2>();
     ea.xy = ctx->xy.as<float2>();
     ea.ell = ctx->ell.as<float4>();
@@ -374,7 +387,8 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
         stats->num_keys = K;
         stats->num_tiles = tiles_total;
         // frame kernel, emit, sort histogram + passes, ranges, raster
-        stats->kernel_launches = (n > 0 ? 1 : 0) + (K > 0 ? 3 + passes : 0) + 1;
+        // frame kernel + view bases, emit, sort histogram + passes, ranges, raster
+        stats->kernel_launches = (n > 0 ? 2 : 0) + (K > 0 ? 3 + passes : 0) + 1;
     }
     return GS_OK;
 }
@@ -488,7 +502,7 @@ int gs_ctx_destroy(gs_ctx* ctx)
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
-                      &ctx->offsets, &ctx->scan_status, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
+                      &ctx->offsets, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
                       &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
     for (DevBuf* b : bufs) b->release();
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
@@ -503,7 +517,7 @@ int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
 {
     if (!ctx) return 0;
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
-                            &ctx->offsets, &ctx->scan_status, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
+                            &ctx->offsets, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
                             &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
     int64_t t = 0;
     for (const DevBuf* b : bufs) t += (int64_t)b->bytes;
@@ -678,29 +692,35 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     ViewParams& v = ctx->h_views[0];
     make_view_params(*cam, *cfg, v);
     const int64_t blocks = (n + 255) / 256;
-    if (ctx->rect.ensure(8 * (size_t)n) || ctx->offsets.ensure(8 * (size_t)n)) return fail(GS_ERR_OOM, "build buffers");
+    if (ctx->rect.ensure(8 * (size_t)n) || ctx->offsets.ensure(4 * (size_t)n)) return fail(GS_ERR_OOM, "build buffers");
     ctx->per_view_capacity = 0;  // rect/offsets may have been regrown: force the frame path to re-check
     if (sizeof(uint64_t) * (size_t)blocks > ctx->scan_status.bytes) {
         if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)blocks, true)) return fail(GS_ERR_OOM, "scan status");
     }
+    if (ctx->view_stats.ensure(sizeof(int64_t) * 2)) return fail(GS_ERR_OOM, "view stats");
+    int64_t* view_total = ctx->view_stats.as<int64_t>();
+    int64_t* view_base = view_total + 1;
     Counters* dc = ctx->counters.as<Counters>();
     GS_CUDA(cudaMemcpyAsync(ctx->views.p, &v, sizeof(ViewParams), cudaMemcpyHostToDevice, st));
     GS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
     FrameArgs fa = {};
     fa.n = n;
+    fa.groups = blocks;
     fa.num_views = 1;
+    fa.views_per_block = 1;
     fa.epoch = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
     fa.num_tiles = blocks;
     fa.views = ctx->views.as<ViewParams>();
     fa.xy = (float2*)d_xy;
     fa.ell = (float4*)d_ellipse;
     fa.rect = ctx->rect.as<int2>();
-    fa.offsets = ctx->offsets.as<int64_t>();
+    fa.offsets = ctx->offsets.as<int32_t>();
     fa.status = ctx->scan_status.as<uint64_t>();
     fa.tile_counter = &dc->frame_tile;
-    fa.total = &dc->total;
+    fa.view_total = view_total;
     fa.err = &dc->err;
     launch_count_stage(fa, st);
+    launch_view_base(view_total, 1, view_base, &dc->total, st);
     GS_CUDA(cudaGetLastError());
     GS_CUDA(cudaMemcpyAsync(ctx->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, st));
     GS_CUDA(cudaStreamSynchronize(st));
@@ -713,8 +733,9 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     ea.n = n;
     ea.num_views = 1;
     ea.views = ctx->views.as<ViewParams>();
-    ea.offsets = ctx->offsets.as<int64_t>();
-    ea.total = &dc->total;
+    ea.offsets = ctx->offsets.as<int32_t>();
+    ea.view_total = view_total;
+    ea.view_base = view_base;
     ea.rect = ctx->rect.as<int2>();
     ea.xy = (const float2*)d_xy;
     ea.ell = (const float4*)d_ellipse;

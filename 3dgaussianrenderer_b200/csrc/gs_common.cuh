@@ -208,19 +208,27 @@ __device__ __forceinline__ Splat project_gaussian(const float4 p, const float4 s
 // ---- SH colour (gaussian_render.cu:50-94; degree 3: cuda_renderer.cu:119-156)
 // sh points at coefficient 0 of this Gaussian, consecutive coefficients
 // `stride` floats apart.
-template <int DEG>
+// G: coefficients in global memory (read-only path) or in shared memory.
+template <bool G>
+__device__ __forceinline__ float ldsh(const float* p)
+{
+    if (G) return __ldg(p);
+    return *p;
+}
+
+template <int DEG, bool G = true>
 __device__ __forceinline__ float3 sh_color(const float x, const float y, const float z, const float* __restrict__ sh,
                                            const int stride)
 {
     float r[3];
 #pragma unroll
-    for (int c = 0; c < 3; ++c) r[c] = 0.0f + 0.282094792F * __ldg(&sh[c * stride]);
+    for (int c = 0; c < 3; ++c) r[c] = 0.0f + 0.282094792F * ldsh<G>(&sh[c * stride]);
     if (DEG > 0) {
         const float b1 = 0.488602512F * y, b2 = 0.488602512F * z, b3 = 0.488602512F * x;
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            r[c] = r[c] + (b1 * __ldg(&sh[(3 + c) * stride]) + b2 * __ldg(&sh[(6 + c) * stride]) +
-                           b3 * __ldg(&sh[(9 + c) * stride]));
+            r[c] = r[c] + (b1 * ldsh<G>(&sh[(3 + c) * stride]) + b2 * ldsh<G>(&sh[(6 + c) * stride]) +
+                           b3 * ldsh<G>(&sh[(9 + c) * stride]));
     }
     if (DEG > 1) {
         const float xx = x * x, yy = y * y;
@@ -231,9 +239,9 @@ __device__ __forceinline__ float3 sh_color(const float x, const float y, const f
         const float b8 = 0.546274215F * (x - y) * (x + y);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            r[c] = r[c] + (b4 * __ldg(&sh[(12 + c) * stride]) + b5 * __ldg(&sh[(15 + c) * stride]) +
-                           b6 * __ldg(&sh[(18 + c) * stride]) + b7 * __ldg(&sh[(21 + c) * stride]) +
-                           b8 * __ldg(&sh[(24 + c) * stride]));
+            r[c] = r[c] + (b4 * ldsh<G>(&sh[(12 + c) * stride]) + b5 * ldsh<G>(&sh[(15 + c) * stride]) +
+                           b6 * ldsh<G>(&sh[(18 + c) * stride]) + b7 * ldsh<G>(&sh[(21 + c) * stride]) +
+                           b8 * ldsh<G>(&sh[(24 + c) * stride]));
     }
     if (DEG > 2) {
         const float xx = x * x, yy = y * y;
@@ -246,10 +254,10 @@ __device__ __forceinline__ float3 sh_color(const float x, const float y, const f
         const float b15 = 0.59004359F * x * (xx - 3.0F * yy);
 #pragma unroll
         for (int c = 0; c < 3; ++c)
-            r[c] = r[c] + (b9 * __ldg(&sh[(27 + c) * stride]) + b10 * __ldg(&sh[(30 + c) * stride]) +
-                           b11 * __ldg(&sh[(33 + c) * stride]) + b12 * __ldg(&sh[(36 + c) * stride]) +
-                           b13 * __ldg(&sh[(39 + c) * stride]) + b14 * __ldg(&sh[(42 + c) * stride]) +
-                           b15 * __ldg(&sh[(45 + c) * stride]));
+            r[c] = r[c] + (b9 * ldsh<G>(&sh[(27 + c) * stride]) + b10 * ldsh<G>(&sh[(30 + c) * stride]) +
+                           b11 * ldsh<G>(&sh[(33 + c) * stride]) + b12 * ldsh<G>(&sh[(36 + c) * stride]) +
+                           b13 * ldsh<G>(&sh[(39 + c) * stride]) + b14 * ldsh<G>(&sh[(42 + c) * stride]) +
+                           b15 * ldsh<G>(&sh[(45 + c) * stride]));
     }
     return make_float3(gclamp(r[0] + 0.5f, 0.0f, 1.0f), gclamp(r[1] + 0.5f, 0.0f, 1.0f),
                        gclamp(r[2] + 0.5f, 0.0f, 1.0f));
@@ -293,6 +301,9 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
                                                      const float y1)
 {
     bool ov = e.cx > x0 && e.cx < x1 && e.cy > y0 && e.cy < y1;
+    // The reference ORs all five tests, so a centre strictly inside the tile
+    // decides the result; skipping the rest changes nothing.
+    if (ov) return true;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
     const float rcy = y0 + (y1 - y0) * 0.5f;
@@ -401,6 +412,43 @@ __device__ __forceinline__ unsigned lanemask_lt()
     unsigned m;
     asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
     return m;
+}
+
+// ---- TMA bulk copy global -> shared (cp.async.bulk, no tensor map) ---------
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+// Arms the barrier for `bytes` and starts one bulk copy completing on it.
+// dst, src and bytes must be multiples of 16.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, uint64_t* bar)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_addr(dst)),
+        "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(phase)
+        : "memory");
+    return ok != 0;
 }
 
 // ---- bounded decoupled look-back ------------------------------------------

@@ -7,30 +7,36 @@ namespace gs {
 
 constexpr int kErrTimeout = 4;  // GS_ERR_DEVICE_TIMEOUT
 
-// Fused SH + projection + count + scan over (view, Gaussian) pairs.
+// Fused SH + projection + count + scan over (view, Gaussian) pairs.  A block
+// owns one group of 256 Gaussians for `views_per_block` consecutive views;
+// every view has its own look-back chain over the groups, so offsets are
+// relative to the view's first key.
 struct FrameArgs {
     int64_t n;          // Gaussians per view
+    int64_t groups;     // ceil(n / 256)
     int32_t num_views;
+    int32_t views_per_block;
     uint32_t epoch;     // look-back epoch of this launch
-    int64_t num_tiles;  // blocks = num_views * ceil(n / 256)
+    int64_t num_tiles;  // blocks = ceil(num_views / views_per_block) * groups
     const float4* pos;
     const float4* sr;
     const float* sh;    // grouped [ceil(n/256)][sh_count][256]
     int32_t sh_count;
     const float4* color_in;  // degree-0 scenes: colour from the model
     const ViewParams* views;
-    // outputs, per view at [view * n + i]
+    // outputs, per view at [view * n + i]; all but offsets only for
+    // Gaussians that overlap at least one tile
     float4* color;
     float2* xy;
     float* z;
     float4* ell;
     float4* conic;
     int2* rect;
-    int64_t* offsets;
+    int32_t* offsets;   // exclusive key offset inside the view
     // scratch
-    uint64_t* status;   // num_tiles words
+    uint64_t* status;   // [num_views][groups] look-back words
     unsigned long long* tile_counter;
-    int64_t* total;
+    int64_t* view_total;  // [num_views] keys per view
     int* err;
 };
 
@@ -38,8 +44,9 @@ struct EmitArgs {
     int64_t n;
     int32_t num_views;
     const ViewParams* views;
-    const int64_t* offsets;
-    const int64_t* total;
+    const int32_t* offsets;
+    const int64_t* view_total;
+    const int64_t* view_base;  // exclusive prefix of view_total
     const int2* rect;
     const float2* xy;
     const float4* ell;
@@ -85,6 +92,8 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
                           float* z, float4* ell, float4* conic, cudaStream_t st);
 void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st);
 void launch_count_stage(const FrameArgs& a, cudaStream_t st);
+// view_base[v] = sum of view_total[u < v]; *total = sum of all.
+void launch_view_base(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total, cudaStream_t st);
 void launch_emit(const EmitArgs& a, cudaStream_t st);
 
 // Sorts num_items pairs on bits [0, key_bits).  When d_num_items is non-null

@@ -3,7 +3,8 @@
 //     projection only), used by the stage API;
 //   * the fused frame kernel: SH colour + EWA projection + tile rectangle +
 //     exact per-Gaussian overlap count (warp-cooperative) + single-pass
-//     decoupled look-back scan of the counts into key offsets;
+//     decoupled look-back scan of the counts into key offsets, for several
+//     views per block so the SH coefficients are read once per group;
 //   * the emit kernel that writes (tile|depth, index) keys at those offsets.
 #include "gs_kernels.h"
 
@@ -29,10 +30,9 @@ __global__ void __launch_bounds__(256) sh_stage_kernel(int64_t n, const float4* 
 }
 
 __global__ void __launch_bounds__(256) project_stage_kernel(int64_t n, const float4* __restrict__ pos,
-                                                            const float4* __restrict__ sr,
-                                                            const ViewParams v, float2* __restrict__ xy,
-                                                            float* __restrict__ z, float4* __restrict__ ell,
-                                                            float4* __restrict__ conic)
+                                                            const float4* __restrict__ sr, const ViewParams v,
+                                                            float2* __restrict__ xy, float* __restrict__ z,
+                                                            float4* __restrict__ ell, float4* __restrict__ conic)
 {
     const int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x;
     if (i >= n) return;
@@ -122,12 +122,13 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
     return hits;
 }
 
-// ---- block scan + decoupled look-back over blocks ----------------------------
+// ---- block scan + decoupled look-back along one chain ---------------------------
 
-// Returns this thread's exclusive offset among all threads of all blocks
-// (ordered by dynamic block id), writes the grand total when last.
-__device__ __forceinline__ int64_t block_offsets(const int hits, const int64_t tile, const int64_t num_tiles,
-                                                 uint64_t* status, const uint32_t epoch, int64_t* total_out, int* err)
+// This thread's exclusive offset within a chain of blocks (`status[0..len)`,
+// block `link` of it); the last block of the chain writes the chain total.
+__device__ __forceinline__ int64_t chain_offsets(const int hits, uint64_t* status, const int64_t link,
+                                                 const int64_t len, const uint32_t epoch, int64_t* chain_total,
+                                                 int* err)
 {
     __shared__ int s_warp[8];
     __shared__ int64_t s_base;
@@ -149,18 +150,20 @@ __device__ __forceinline__ int64_t block_offsets(const int hits, const int64_t t
         }
         const uint64_t agg = (uint64_t)run;
         uint64_t excl = 0;
-        if (tile == 0) {
+        if (link == 0) {
             store_status(status, status_word(kFlagP, epoch, agg));
         } else {
-            store_status(status + tile, status_word(kFlagA, epoch, agg));
-            excl = look_back(status, tile, 1, epoch, err, kErrTimeout);
-            store_status(status + tile, status_word(kFlagP, epoch, excl + agg));
+            store_status(status + link, status_word(kFlagA, epoch, agg));
+            excl = look_back(status, link, 1, epoch, err, kErrTimeout);
+            store_status(status + link, status_word(kFlagP, epoch, excl + agg));
         }
         s_base = (int64_t)excl;
-        if (tile == num_tiles - 1) *total_out = (int64_t)(excl + agg);
+        if (link == len - 1) *chain_total = (int64_t)(excl + agg);
     }
     __syncthreads();
-    return s_base + s_warp[warp] + (incl - hits);
+    const int64_t r = s_base + s_warp[warp] + (incl - hits);
+    __syncthreads();  // s_warp / s_base are reused by the next call
+    return r;
 }
 
 __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
@@ -168,58 +171,98 @@ __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
     __shared__ int64_t s_tile;
     if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(counter, 1ull);
     __syncthreads();
-    return s_tile;
+    const int64_t t = s_tile;
+    return t;
 }
 
 // ---- fused frame kernel ------------------------------------------------------
 //
-// One 256-thread block per (view, group of 256 Gaussians), blocks taken in
-// a dynamic order so the look-back never waits on an unscheduled block.
-// Per Gaussian it reads position, scale/rotation and (DEG >= 0) the group's
-// SH coefficients (DEG = -1: degree-0 scene, colour copied from the model), and writes colour, clip centre, depth, ellipse, conic,
-// packed tile rectangle and the exclusive key offset.
+// Block `tile` (taken in dynamic order, so a look-back only ever waits on a
+// block that is already running) owns group g = tile % groups for views
+// [c*vpb, (c+1)*vpb), c = tile / groups.  It reads position and
+// scale/rotation of its 256 Gaussians once and, for SH scenes, brings the
+// group's coefficients (the first 3*(DEG+1)^2 rows of the grouped layout,
+// contiguous) into shared memory with one TMA bulk copy.  Then per view:
+// SH colour, projection, tile rectangle, exact overlap count, and the
+// within-view key offset from that view's look-back chain.  Gaussians that
+// overlap no tile write only their offset.
 template <int DEG>
 __global__ void __launch_bounds__(256) frame_project_kernel(FrameArgs a)
 {
+    extern __shared__ __align__(128) float s_sh[];  // [3*(DEG+1)^2][256]
+    __shared__ __align__(8) uint64_t s_bar;
     const int64_t tile = acquire_tile(a.tile_counter);
-    const int64_t groups = (a.n + 255) / 256;
-    const int view = (int)(tile / groups);
-    const int64_t group = tile - (int64_t)view * groups;
+    const int64_t chunk = tile / a.groups;
+    const int64_t group = tile - chunk * a.groups;
     const int64_t i = group * 256 + threadIdx.x;
     const bool valid = i < a.n;
-    const ViewParams& v = a.views[view];
-    const int64_t o = (int64_t)view * a.n + i;  // per-view output index
+    const int v0 = (int)chunk * a.views_per_block;
+    const int v1 = min(a.num_views, v0 + a.views_per_block);
+    constexpr int NCOEF = DEG >= 0 ? 3 * (DEG + 1) * (DEG + 1) : 0;
 
-    Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-    int4 r = make_int4(0, 0, 0, 0);
-    int cand = 0;
-    if (valid) {
-        const float4 p = __ldg(&a.pos[i]);
-        const float4 sr = __ldg(&a.sr[i]);
-        if (DEG >= 0) {
-            const float3 d = view_dir(v, p);
-            const float3 c = sh_color<DEG>(d.x, d.y, d.z, a.sh + group * 256 * a.sh_count + threadIdx.x, 256);
-            a.color[o] = make_float4(c.x, c.y, c.z, p.w);
-        } else {
-            a.color[o] = __ldg(&a.color_in[i]);
+    if (DEG >= 0) {
+        if (threadIdx.x == 0) {
+            mbar_init(&s_bar, 1);
+            bulk_load(s_sh, a.sh + group * 256 * (int64_t)a.sh_count, NCOEF * 256 * sizeof(float), &s_bar);
         }
-        const Splat s = project_gaussian(p, sr, v);
-        a.xy[o] = make_float2(s.x, s.y);
-        a.z[o] = s.z;
-        a.ell[o] = make_float4(s.cs, s.sn, s.ex, s.ey);
-        a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
-        e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
-        r = tile_rect(e, v);
-        cand = rect_candidates(r);
-        a.rect[o] = pack_rect(r);
     }
-    const int hits = warp_count_hits(e, r, cand, v);
-    const int64_t off = block_offsets(hits, tile, a.num_tiles, a.status, a.epoch, a.total, a.err);
-    if (valid) a.offsets[o] = off;
+    float4 p = make_float4(0.f, 0.f, 0.f, 0.f), sr = p, cin = p;
+    if (valid) {
+        p = __ldg(&a.pos[i]);
+        sr = __ldg(&a.sr[i]);
+        if (DEG < 0) cin = __ldg(&a.color_in[i]);
+    }
+    if (DEG >= 0) {
+        __syncthreads();  // barrier initialised before anyone polls it
+        int spins = 0;
+        while (!mbar_try_wait(&s_bar, 0)) {
+            if (++spins > kSpinLimit) {
+                // a bulk copy from valid device memory always lands; report
+                // and carry on (the frame is discarded by the host)
+                if (threadIdx.x == 0) atomicCAS(a.err, 0, kErrTimeout);
+                break;
+            }
+        }
+    }
+
+    for (int view = v0; view < v1; ++view) {
+        const ViewParams& v = a.views[view];
+        const int64_t o = (int64_t)view * a.n + i;
+        Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        int4 r = make_int4(0, 0, 0, 0);
+        int cand = 0;
+        Splat s;
+        float4 col = cin;
+        if (valid) {
+            if (DEG >= 0) {
+                const float3 d = view_dir(v, p);
+                const float3 c = sh_color<DEG, false>(d.x, d.y, d.z, s_sh + threadIdx.x, 256);
+                col = make_float4(c.x, c.y, c.z, p.w);
+            }
+            s = project_gaussian(p, sr, v);
+            e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
+            r = tile_rect(e, v);
+            cand = rect_candidates(r);
+        }
+        const int hits = warp_count_hits(e, r, cand, v);
+        const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, a.epoch,
+                                          a.view_total + view, a.err);
+        if (valid) {
+            a.offsets[o] = (int32_t)off;
+            if (hits > 0) {
+                a.color[o] = col;
+                a.xy[o] = make_float2(s.x, s.y);
+                a.z[o] = s.z;
+                a.ell[o] = make_float4(s.cs, s.sn, s.ex, s.ey);
+                a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
+                a.rect[o] = pack_rect(r);
+            }
+        }
+    }
 }
 
 // Count-only variant for the stage API: rectangle + exact count + scan from
-// already projected (xy, ellipse) in the reference layouts.
+// already projected (xy, ellipse) in the reference layouts (one view).
 __global__ void __launch_bounds__(256) count_stage_kernel(FrameArgs a)
 {
     const int64_t tile = acquire_tile(a.tile_counter);
@@ -238,17 +281,29 @@ __global__ void __launch_bounds__(256) count_stage_kernel(FrameArgs a)
         a.rect[i] = pack_rect(r);
     }
     const int hits = warp_count_hits(e, r, cand, v);
-    const int64_t off = block_offsets(hits, tile, a.num_tiles, a.status, a.epoch, a.total, a.err);
-    if (valid) a.offsets[i] = off;
+    const int64_t off = chain_offsets(hits, a.status, tile, a.groups, a.epoch, a.view_total, a.err);
+    if (valid) a.offsets[i] = (int32_t)off;
+}
+
+__global__ void view_base_kernel(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total)
+{
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        int64_t run = 0;
+        for (int v = 0; v < num_views; ++v) {
+            view_base[v] = run;
+            run += view_total[v];
+        }
+        *total = run;
+    }
 }
 
 // ---- emit -------------------------------------------------------------------
 //
 // Rewalks each warp's candidates and writes every hit at
-// offsets[g] + (number of earlier hits of g), so keys leave in Gaussian
-// order with tiles ascending inside a Gaussian; a stable sort then breaks
-// equal keys by index.  The key holds the global tile id (view tile offset
-// + tile) and the value the per-view-flattened Gaussian index.
+// view_base + offsets[g] + (number of earlier hits of g), so keys leave in
+// (view, Gaussian) order with tiles ascending inside a Gaussian; a stable
+// sort then breaks equal keys by index.  The key holds the global tile id
+// (view tile offset + tile), the value the view-flattened Gaussian index.
 __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
 {
     const int64_t gi = (int64_t)blockIdx.x * 256 + threadIdx.x;  // over views * n
@@ -264,9 +319,11 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
     float depth = 0.f;
     int64_t off = 0;
     if (valid) {
-        off = a.offsets[gi];
-        const int64_t next = (gi + 1 < total_items) ? a.offsets[gi + 1] : *a.total;
-        hits = (int)(next - off);
+        const int64_t i = gi - (int64_t)view * a.n;
+        const int64_t own = a.offsets[gi];
+        const int64_t next = (i + 1 < a.n) ? (int64_t)a.offsets[gi + 1] : a.view_total[view];
+        hits = (int)(next - own);
+        off = a.view_base[view] + own;
         if (hits > 0) {
             r = unpack_rect(a.rect[gi]);
             cand = rect_candidates(r);
@@ -341,16 +398,28 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
     project_stage_kernel<<<grid, 256, 0, st>>>(n, pos, sr, v, xy, z, ell, conic);
 }
 
+template <int DEG>
+static void launch_frame_deg(const FrameArgs& a, cudaStream_t st)
+{
+    constexpr int NCOEF = DEG >= 0 ? 3 * (DEG + 1) * (DEG + 1) : 0;
+    constexpr int smem = NCOEF * 256 * (int)sizeof(float);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(frame_project_kernel<DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    frame_project_kernel<DEG><<<(unsigned)a.num_tiles, 256, smem, st>>>(a);
+}
+
 void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st)
 {
-    const unsigned grid = (unsigned)a.num_tiles;
-    if (grid == 0) return;
+    if (a.num_tiles == 0) return;
     switch (deg) {
-        case -1: frame_project_kernel<-1><<<grid, 256, 0, st>>>(a); break;
-        case 0: frame_project_kernel<0><<<grid, 256, 0, st>>>(a); break;
-        case 1: frame_project_kernel<1><<<grid, 256, 0, st>>>(a); break;
-        case 2: frame_project_kernel<2><<<grid, 256, 0, st>>>(a); break;
-        default: frame_project_kernel<3><<<grid, 256, 0, st>>>(a); break;
+        case -1: launch_frame_deg<-1>(a, st); break;
+        case 0: launch_frame_deg<0>(a, st); break;
+        case 1: launch_frame_deg<1>(a, st); break;
+        case 2: launch_frame_deg<2>(a, st); break;
+        default: launch_frame_deg<3>(a, st); break;
     }
 }
 
@@ -359,6 +428,11 @@ void launch_count_stage(const FrameArgs& a, cudaStream_t st)
     const unsigned grid = (unsigned)a.num_tiles;
     if (grid == 0) return;
     count_stage_kernel<<<grid, 256, 0, st>>>(a);
+}
+
+void launch_view_base(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total, cudaStream_t st)
+{
+    view_base_kernel<<<1, 32, 0, st>>>(view_total, num_views, view_base, total);
 }
 
 void launch_emit(const EmitArgs& a, cudaStream_t st)

@@ -1,17 +1,24 @@
 // Tile rasteriser (replaces rasterizeTilesKernel, core/gaussian_render.cu:679-775).
 //
-// One CTA per tile, one thread per pixel.  The tile's depth-sorted entries
-// are consumed in batches of one entry per thread: every thread gathers one
-// splat (centre, conic + opacity, colour) into shared memory, then every
-// pixel blends the whole batch front to back in FP32.
+// One CTA per tile, one thread per pixel; each warp owns an 8x4 block of
+// the tile.  The tile's depth-sorted entries are consumed in batches of one
+// entry per thread: every thread gathers one splat (centre, conic + opacity,
+// colour) into shared memory, then the pixels blend the batch front to
+// back in FP32 with the reference's arithmetic.
 //
 // Termination:
-//  * GS_TERM_REFERENCE: after every 32nd entry of the tile's list the CTA
-//    stops once no in-image pixel has T > 0.02 (the reference's test at
-//    :745, at the same 32-entry granularity whatever the batch size).
-//  * GS_TERM_TMIN: a pixel stops once its T < t_min; a warp whose pixels
-//    are all done skips the batch (warp ballot), the CTA stops when every
-//    pixel is done.
+//  * GS_TERM_REFERENCE: every pixel evaluates every entry; after every 32nd
+//    entry of the tile's list the CTA stops once no in-image pixel has
+//    T > 0.02 (the reference's test at :745, at the same granularity
+//    whatever the batch size).  Bit-identical to the reference kernel.
+//  * GS_TERM_TMIN: a pixel stops once its T < t_min; a warp whose pixels are
+//    all done skips the rest (warp ballot), the CTA stops when every pixel
+//    is done.  Each warp first tests 32 staged splats at a time against its
+//    8x4 pixel block (one splat per lane) and blends only the survivors
+//    (ballot compaction).  A splat survives when its cutoff ellipse, where
+//    opacity * exp(-q/2) = kCullAlpha, touches the block; the contributions
+//    skipped are each below kCullAlpha (2^-18), so a pixel needs more than a
+//    thousand of them to move by 1/255.
 //
 // The plain path launches one CTA per tile; the batched path runs a
 // persistent grid that pulls global tile ids (all views' tiles, flattened)
@@ -22,17 +29,42 @@
 
 namespace gs {
 
+constexpr float kCullAlpha = 3.814697265625e-06f;  // 2^-18
+
+struct RasterSmem {
+    float2* xy;
+    float4* con;  // (a, b, c, opacity)
+    float4* col;
+    float4* box;  // cutoff box (x0, x1, y0, y1), GS_TERM_TMIN only
+};
+
+__device__ __forceinline__ void blend(const float cx, const float cy, const float2 c, const float4 k, const float4 col,
+                                      float& r, float& g, float& b, float& T)
+{
+    const float dx = cx - c.x, dy = cy - c.y;
+    const float q = k.x * dx * dx + k.z * dy * dy + 2.0f * k.y * dx * dy;
+    const float density = __expf(-0.5f * q);
+    const float alpha = k.w * __saturatef(density);
+    r += col.x * T * alpha;
+    g += col.y * T * alpha;
+    b += col.z * T * alpha;
+    T *= (1.0f - alpha);
+}
+
 template <int TW, int TH, int MODE>
 __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParams& v, const int64_t gtile,
-                                            const int local_tile, float2* s_xy, float4* s_con, float4* s_col)
+                                            const int local_tile, const RasterSmem& sm)
 {
     constexpr int NT = TW * TH;
+    constexpr int WX = TW / 8;  // warps per tile row
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int first = __ldg(&a.ranges[2 * gtile]);
     const int last = __ldg(&a.ranges[2 * gtile + 1]);
     const int count = last - first;
     const int tx = local_tile % v.tiles_x, ty = local_tile / v.tiles_x;
-    const int px = tx * TW + (int)(threadIdx.x % TW);
-    const int py = ty * TH + (int)(threadIdx.x / TW);
+    const int wx0 = tx * TW + (warp % WX) * 8, wy0 = ty * TH + (warp / WX) * 4;
+    const int px = wx0 + (lane & 7);
+    const int py = wy0 + (lane >> 3);
     const bool inimg = px < v.width && py < v.height;
     if (count <= 0) {
         // the reference clears the image and skips empty tiles (main.cpp:363);
@@ -43,6 +75,9 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
     // pixel corner sample, gaussian_render.cu:701-704
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy = (float)py * v.texel_y - 1.0f;
+    // this warp's 8x4 block in clip space
+    const float bx0 = (float)wx0 * v.texel_x - 1.0f, bx1 = (float)(wx0 + 7) * v.texel_x - 1.0f;
+    const float by0 = (float)wy0 * v.texel_y - 1.0f, by1 = (float)(wy0 + 3) * v.texel_y - 1.0f;
 
     float r = 0.0f, g = 0.0f, b = 0.0f;
     float T = 1.0f;
@@ -55,25 +90,30 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
             const int s = __ldg(&a.values[first + base + threadIdx.x]);
             const float4 col = __ldg(&a.color[s]);
             const float4 con = __ldg(&a.conic[s]);
-            s_xy[threadIdx.x] = __ldg(&a.xy[s]);
-            s_con[threadIdx.x] = make_float4(con.x, con.y, con.z, col.w);
-            s_col[threadIdx.x] = col;
+            const float2 c = __ldg(&a.xy[s]);
+            sm.xy[threadIdx.x] = c;
+            sm.con[threadIdx.x] = make_float4(con.x, con.y, con.z, col.w);
+            sm.col[threadIdx.x] = col;
+            if (MODE == 1) {
+                float4 box;
+                const float det = con.x * con.z - con.y * con.y;
+                if (!(col.w > kCullAlpha)) {
+                    box = make_float4(1e30f, -1e30f, 1e30f, -1e30f);  // contributes nothing
+                } else if (!(det > 0.0f) || !(con.x > 0.0f) || !(con.z > 0.0f)) {
+                    box = make_float4(-1e30f, 1e30f, -1e30f, 1e30f);  // degenerate: never cull
+                } else {
+                    const float qc = 2.0f * logf(col.w / kCullAlpha);
+                    const float ex = sqrtf(qc * con.z / det), ey = sqrtf(qc * con.x / det);
+                    box = make_float4(c.x - ex, c.x + ex, c.y - ey, c.y + ey);
+                }
+                sm.box[threadIdx.x] = box;
+            }
         }
         __syncthreads();
         if (MODE == 0) {
             bool stop = false;
             for (int j = 0; j < nb; ++j) {
-                const float2 c = s_xy[j];
-                const float4 k = s_con[j];
-                const float4 col = s_col[j];
-                const float dx = cx - c.x, dy = cy - c.y;
-                const float q = k.x * dx * dx + k.z * dy * dy + 2.0f * k.y * dx * dy;
-                const float density = __expf(-0.5f * q);
-                const float alpha = k.w * __saturatef(density);
-                r += col.x * T * alpha;
-                g += col.y * T * alpha;
-                b += col.z * T * alpha;
-                T *= (1.0f - alpha);
+                blend(cx, cy, sm.xy[j], sm.con[j], sm.col[j], r, g, b, T);
                 const int e = base + j + 1;
                 if ((e & 31) == 0 || e == count) {
                     if (__syncthreads_count(inimg && T > 0.02f) == 0) {
@@ -84,20 +124,20 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
             }
             if (stop) break;
         } else {
-            if (__any_sync(kFull, !done)) {
-                for (int j = 0; j < nb; ++j) {
+            for (int c0 = 0; c0 < nb; c0 += 32) {
+                if (__all_sync(kFull, done)) break;
+                const int j = c0 + lane;
+                bool keep = false;
+                if (j < nb) {
+                    const float4 bx = sm.box[j];
+                    keep = bx.x <= bx1 && bx.y >= bx0 && bx.z <= by1 && bx.w >= by0;
+                }
+                unsigned m = __ballot_sync(kFull, keep);
+                while (m) {
+                    const int k = c0 + __ffs(m) - 1;
+                    m &= m - 1;
                     if (!done) {
-                        const float2 c = s_xy[j];
-                        const float4 k = s_con[j];
-                        const float4 col = s_col[j];
-                        const float dx = cx - c.x, dy = cy - c.y;
-                        const float q = k.x * dx * dx + k.z * dy * dy + 2.0f * k.y * dx * dy;
-                        const float density = __expf(-0.5f * q);
-                        const float alpha = k.w * __saturatef(density);
-                        r += col.x * T * alpha;
-                        g += col.y * T * alpha;
-                        b += col.z * T * alpha;
-                        T *= (1.0f - alpha);
+                        blend(cx, cy, sm.xy[k], sm.con[k], sm.col[k], r, g, b, T);
                         if (T < a.t_min) done = true;
                     }
                 }
@@ -122,8 +162,9 @@ __global__ void __launch_bounds__(TW * TH) raster_kernel(RasterArgs a)
     __shared__ float2 s_xy[TW * TH];
     __shared__ float4 s_con[TW * TH];
     __shared__ float4 s_col[TW * TH];
-    raster_tile<TW, TH, MODE>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, s_xy, s_con,
-                              s_col);
+    __shared__ float4 s_box[MODE == 1 ? TW * TH : 1];
+    const RasterSmem sm = {s_xy, s_con, s_col, s_box};
+    raster_tile<TW, TH, MODE>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, sm);
 }
 
 // Persistent variant over the flattened tiles of all views.
@@ -133,18 +174,26 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
     __shared__ float2 s_xy[TW * TH];
     __shared__ float4 s_con[TW * TH];
     __shared__ float4 s_col[TW * TH];
+    __shared__ float4 s_box[MODE == 1 ? TW * TH : 1];
     __shared__ int64_t s_tile;
+    const RasterSmem sm = {s_xy, s_con, s_col, s_box};
     for (;;) {
         __syncthreads();
         if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(a.tile_counter, 1ull);
         __syncthreads();
         const int64_t gtile = s_tile;
         if (gtile >= a.num_tiles_total) return;
-        // view owning this tile: views are few, a linear scan is enough
-        int view = 0;
-        while (view + 1 < a.num_views && a.views[view + 1].tile_offset <= gtile) ++view;
-        const ViewParams& v = a.views[view];
-        raster_tile<TW, TH, MODE>(a, v, gtile, (int)(gtile - v.tile_offset), s_xy, s_con, s_col);
+        // view owning this tile: binary search over the views' first tiles
+        int lo = 0, hi = a.num_views - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.views[mid].tile_offset <= gtile)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const ViewParams& v = a.views[lo];
+        raster_tile<TW, TH, MODE>(a, v, gtile, (int)(gtile - v.tile_offset), sm);
     }
 }
 

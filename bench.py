@@ -188,40 +188,42 @@ def run_ours(args, rank, world, local_rank):
 
     # e2e through the public host-buffer API: camera upload + images back to pinned host memory
     total_bytes = sum(c.GetWidth() * c.GetHeight() * 4 for c in cams)
-    host = torch.empty(total_bytes, dtype=torch.uint8).pin_memory()
-    host_np = host.numpy()
-    for _ in range(max(1, args.warmup // 2)):
-        gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    t0 = time.perf_counter()
-    f0 = torch.cuda.Event(enable_timing=True)
-    f1 = torch.cuda.Event(enable_timing=True)
-    f0.record(stream)
-    for _ in range(args.steps):
-        gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
-    f1.record(stream)
-    torch.cuda.synchronize()
-    e2e_ms = f0.elapsed_time(f1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * VIEWS * args.steps / (float(t.item()) / 1e3)
+    e2e_value = None
+    if not args.no_e2e:
+        host = torch.empty(total_bytes, dtype=torch.uint8).pin_memory()
+        host_np = host.numpy()
+        for _ in range(max(1, args.warmup // 2)):
+            gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        f0 = torch.cuda.Event(enable_timing=True)
+        f1 = torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        for _ in range(args.steps):
+            gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
+        f1.record(stream)
+        torch.cuda.synchronize()
+        t = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_value = world * VIEWS * args.steps / (float(t.item()) / 1e3)
 
     # plain single-view path over the same views (for the batched/plain ratio)
-    plain_views = min(VIEWS, 16)
-    for v in range(2):
-        gs.render(ctx, scene, cams[v], rc, outs[v], stream)
-    torch.cuda.synchronize()
-    g0 = torch.cuda.Event(enable_timing=True)
-    g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(stream)
-    for v in range(plain_views):
-        gs.render(ctx, scene, cams[v], rc, outs[v], stream)
-    g1.record(stream)
-    torch.cuda.synchronize()
-    plain_value = plain_views / (g0.elapsed_time(g1) / 1e3)
+    plain_value = None
+    if not args.no_plain:
+        plain_views = min(VIEWS, 16)
+        for v in range(2):
+            gs.render(ctx, scene, cams[v], rc, outs[v], stream)
+        torch.cuda.synchronize()
+        g0 = torch.cuda.Event(enable_timing=True)
+        g1 = torch.cuda.Event(enable_timing=True)
+        g0.record(stream)
+        for v in range(plain_views):
+            gs.render(ctx, scene, cams[v], rc, outs[v], stream)
+        g1.record(stream)
+        torch.cuda.synchronize()
+        plain_value = plain_views / (g0.elapsed_time(g1) / 1e3)
 
     if rank != 0:
         return
@@ -269,7 +271,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--no-plain", action="store_true", help="skip the single-view leg (profiling runs)")
+    ap.add_argument("--views", type=int, default=VIEWS,
+                    help="views per batched frame (64 = the workload; fewer only for small profiling cases)")
     args = ap.parse_args()
+    globals()["VIEWS"] = args.views
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
