@@ -416,4 +416,140 @@ def stage_raster(cam: Camera, cfg: RenderConfig, d_ranges, d_values, d_xy, d_con
                               _ptr(d_conic), _ptr(d_color), _ptr(d_rgba), _stream_ptr(stream)), "gs_stage_raster")
 
 
+# ---------------------------------------------------------------------------
+# Serving (continuous batching over resident scenes)
+# ---------------------------------------------------------------------------
+
+class gs_server_cfg(ctypes.Structure):
+    _fields_ = [
+        ("budget_bytes", ctypes.c_int64),
+        ("max_batch_views", ctypes.c_int32),
+        ("num_workers", ctypes.c_int32),
+        ("render", gs_render_cfg),
+    ]
+
+
+class gs_server_stats(ctypes.Structure):
+    _fields_ = [
+        ("views_done", ctypes.c_int64),
+        ("batches_done", ctypes.c_int64),
+        ("max_batch", ctypes.c_int64),
+        ("p50_ms", ctypes.c_double),
+        ("p99_ms", ctypes.c_double),
+        ("mean_ms", ctypes.c_double),
+        ("views_per_s", ctypes.c_double),
+        ("resident_bytes", ctypes.c_int64),
+        ("frame_bytes", ctypes.c_int64),
+        ("pending", ctypes.c_int64),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_sig("gs_server_default_cfg", None, ctypes.POINTER(gs_server_cfg))
+_sig("gs_server_create", _I, _I, ctypes.POINTER(gs_server_cfg), ctypes.POINTER(_P))
+_sig("gs_server_destroy", _I, _P)
+_sig("gs_server_add_scene", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.POINTER(_I32))
+_sig("gs_server_submit", _I, _P, _I32, ctypes.POINTER(gs_camera), _P, ctypes.POINTER(_I64))
+_sig("gs_server_wait", _I, _P, _I64, ctypes.c_double, ctypes.POINTER(ctypes.c_double))
+_sig("gs_server_get_stats", _I, _P, ctypes.POINTER(gs_server_stats))
+_sig("gs_server_reset_stats", _I, _P)
+_sig("gs_ply_info", _I, ctypes.c_char_p, ctypes.POINTER(_I64), ctypes.POINTER(_I32))
+_sig("gs_ply_last_error", ctypes.c_char_p)
+_sig("gs_ply_read", _I, ctypes.c_char_p, _P, _P, _P, _P, _P)
+_sig("gs_ply_write", _I, ctypes.c_char_p, _I64, _P, _P, _P, _P, _I32)
+
+
+class Server:
+    """Continuous-batching server (gs_server_*): resident scenes, requests
+    from any thread, batched frames formed as workers free up."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 150 << 30, max_batch_views: int = 16,
+                 num_workers: int = 2, cfg: RenderConfig | None = None):
+        c = gs_server_cfg()
+        lib.gs_server_default_cfg(ctypes.byref(c))
+        c.budget_bytes = budget_bytes
+        c.max_batch_views = max_batch_views
+        c.num_workers = num_workers
+        if cfg is not None:
+            c.render = cfg.c()
+        h = _P()
+        check(lib.gs_server_create(device, ctypes.byref(c), ctypes.byref(h)), "gs_server_create")
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib.gs_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, pos4, sr4, sh_grouped, sh_degree, color4=None) -> int:
+        pos4 = np.ascontiguousarray(pos4, np.float32)
+        sr4 = np.ascontiguousarray(sr4, np.float32)
+        sh = None if sh_grouped is None else np.ascontiguousarray(sh_grouped, np.float32)
+        col = None if color4 is None else np.ascontiguousarray(color4, np.float32)
+        sid = _I32(0)
+        check(lib.gs_server_add_scene(self.h, pos4.shape[0], _ptr(pos4), _ptr(sr4), _ptr(col), _ptr(sh), sh_degree,
+                                      ctypes.byref(sid)), "gs_server_add_scene")
+        return int(sid.value)
+
+    def submit(self, scene_id: int, cam: Camera, out: np.ndarray) -> int:
+        rid = _I64(0)
+        check(lib.gs_server_submit(self.h, scene_id, ctypes.byref(cam.c), _ptr(out), ctypes.byref(rid)),
+              "gs_server_submit")
+        return int(rid.value)
+
+    def wait(self, rid: int, timeout_ms: float = 60_000.0) -> float:
+        lat = ctypes.c_double(0)
+        check(lib.gs_server_wait(self.h, rid, timeout_ms, ctypes.byref(lat)), "gs_server_wait")
+        return float(lat.value)
+
+    def stats(self) -> dict:
+        s = gs_server_stats()
+        check(lib.gs_server_get_stats(self.h, ctypes.byref(s)), "gs_server_get_stats")
+        return s.as_dict()
+
+    def reset_stats(self):
+        check(lib.gs_server_reset_stats(self.h), "gs_server_reset_stats")
+
+
+# ---------------------------------------------------------------------------
+# PLY (parsePly / savePly)
+# ---------------------------------------------------------------------------
+
+def load_ply(path: str) -> dict:
+    """Reads a 3DGS PLY with the reference's load transforms; returns a scene
+    dict (pos4, sr4, color4, sh_grouped, sh_degree, n, bounds)."""
+    n = _I64(0)
+    deg = _I32(0)
+    if lib.gs_ply_info(path.encode(), ctypes.byref(n), ctypes.byref(deg)) != GS_OK:
+        raise ValueError(lib.gs_ply_last_error().decode())
+    n, deg = int(n.value), int(deg.value)
+    pos4 = np.zeros((n, 4), np.float32)
+    sr4 = np.zeros((n, 4), np.float32)
+    color4 = np.zeros((n, 4), np.float32)
+    groups = (n + 255) // 256
+    sh = np.zeros(groups * 256 * 3 * (deg + 1) ** 2, np.float32) if deg > 0 else None
+    bounds = np.zeros(6, np.float32)
+    if lib.gs_ply_read(path.encode(), _ptr(pos4), _ptr(sr4), _ptr(color4), _ptr(sh), _ptr(bounds)) != GS_OK:
+        raise ValueError(lib.gs_ply_last_error().decode())
+    return {"pos4": pos4, "sr4": sr4, "color4": color4, "sh_grouped": sh, "sh_degree": deg, "n": n,
+            "bounds": bounds}
+
+
+def save_ply(path: str, pos4, sr4, color4, sh_grouped, sh_degree: int):
+    pos4 = np.ascontiguousarray(pos4, np.float32)
+    sr4 = np.ascontiguousarray(sr4, np.float32)
+    col = None if color4 is None else np.ascontiguousarray(color4, np.float32)
+    sh = None if sh_grouped is None else np.ascontiguousarray(sh_grouped, np.float32)
+    check(lib.gs_ply_write(path.encode(), pos4.shape[0], _ptr(pos4), _ptr(sr4), _ptr(col), _ptr(sh), sh_degree),
+          "gs_ply_write")
+
+
 from . import scenes  # noqa: E402,F401

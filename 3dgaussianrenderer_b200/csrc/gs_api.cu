@@ -107,6 +107,7 @@ struct gs_ctx {
     uint32_t epoch_scan = 1, epoch_sort = 1;
     DevBuf views;                          // ViewParams[]
     DevBuf color, xy, z, ell, conic, rect, offsets;  // per (view, Gaussian)
+    DevBuf rec, hitmask;                   // T_min raster records (48 B), candidate hit masks
     DevBuf scan_status;                    // frame kernel look-back words, [view][group]
     DevBuf view_stats;                     // int64 [2][views]: keys per view, first key of view
     DevBuf keys0, vals0, keys1, vals1;     // tile lists
@@ -248,7 +249,8 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     if (items > ctx->per_view_capacity) {
         const size_t m = (size_t)items;
         if (ctx->color.ensure(16 * m) || ctx->xy.ensure(8 * m) || ctx->z.ensure(4 * m) || ctx->ell.ensure(16 * m) ||
-            ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(4 * m))
+            ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(4 * m) ||
+            ctx->rec.ensure(48 * m) || ctx->hitmask.ensure(4 * m))
             return fail(GS_ERR_OOM, "splat buffers");
         ctx->per_view_capacity = items;
     }
@@ -286,6 +288,9 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     fa.ell = ctx->ell.as<float4>();
     fa.conic = ctx->conic.as<float4>();
     fa.rect = ctx->rect.as<int2>();
+    fa.rec = ctx->rec.as<float4>();
+    fa.hitmask = ctx->hitmask.as<uint32_t>();
+    fa.raster_mode = cfg.termination;
     fa.offsets = ctx->offsets.as<int32_t>();
     fa.status = ctx->scan_status.as<uint64_t>();
     fa.tile_counter = &dc->frame_tile;
@@ -325,6 +330,7 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     ea.view_total = view_total;
     ea.view_base = view_base;
     ea.rect = ctx->rect.as<int2>();
+    ea.hitmask = ctx->hitmask.as<uint32_t>();
     ea.xy = ctx->xy.as<float2>();
     ea.ell = ctx->ell.as<float4>();
     ea.z = ctx->z.as<float>();
@@ -368,6 +374,7 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     ra.xy = ctx->xy.as<float2>();
     ra.conic = ctx->conic.as<float4>();
     ra.color = ctx->color.as<float4>();
+    ra.rec = cfg.termination == GS_TERM_TMIN ? ctx->rec.as<float4>() : nullptr;
     ra.t_min = cfg.t_min;
     ra.tile_counter = &dc->raster_tile;
     launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, num_views > 1, ctx->num_sms, st);
@@ -502,7 +509,7 @@ int gs_ctx_destroy(gs_ctx* ctx)
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
     DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
-                      &ctx->offsets, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
+                      &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
                       &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
     for (DevBuf* b : bufs) b->release();
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
@@ -517,7 +524,7 @@ int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
 {
     if (!ctx) return 0;
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
-                            &ctx->offsets, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
+                            &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
                             &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
     int64_t t = 0;
     for (const DevBuf* b : bufs) t += (int64_t)b->bytes;
@@ -692,7 +699,8 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     ViewParams& v = ctx->h_views[0];
     make_view_params(*cam, *cfg, v);
     const int64_t blocks = (n + 255) / 256;
-    if (ctx->rect.ensure(8 * (size_t)n) || ctx->offsets.ensure(4 * (size_t)n)) return fail(GS_ERR_OOM, "build buffers");
+    if (ctx->rect.ensure(8 * (size_t)n) || ctx->offsets.ensure(4 * (size_t)n) || ctx->hitmask.ensure(4 * (size_t)n))
+        return fail(GS_ERR_OOM, "build buffers");
     ctx->per_view_capacity = 0;  // rect/offsets may have been regrown: force the frame path to re-check
     if (sizeof(uint64_t) * (size_t)blocks > ctx->scan_status.bytes) {
         if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)blocks, true)) return fail(GS_ERR_OOM, "scan status");
@@ -714,6 +722,7 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     fa.xy = (float2*)d_xy;
     fa.ell = (float4*)d_ellipse;
     fa.rect = ctx->rect.as<int2>();
+    fa.hitmask = ctx->hitmask.as<uint32_t>();
     fa.offsets = ctx->offsets.as<int32_t>();
     fa.status = ctx->scan_status.as<uint64_t>();
     fa.tile_counter = &dc->frame_tile;
@@ -737,6 +746,7 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     ea.view_total = view_total;
     ea.view_base = view_base;
     ea.rect = ctx->rect.as<int2>();
+    ea.hitmask = ctx->hitmask.as<uint32_t>();
     ea.xy = (const float2*)d_xy;
     ea.ell = (const float4*)d_ellipse;
     ea.z = d_z;

@@ -24,14 +24,17 @@ struct FrameArgs {
     int32_t sh_count;
     const float4* color_in;  // degree-0 scenes: colour from the model
     const ViewParams* views;
-    // outputs, per view at [view * n + i]; all but offsets only for
-    // Gaussians that overlap at least one tile
+    // outputs, per view at [view * n + i]; offsets for every Gaussian, the
+    // rest only for Gaussians that overlap at least one tile
+    int32_t raster_mode;  // GS_TERM_REFERENCE: color/xy/conic; GS_TERM_TMIN: rec
     float4* color;
-    float2* xy;
+    float2* xy;         // reference mode, or any mode when the rectangle has > 32 candidates
     float* z;
-    float4* ell;
+    float4* ell;        // only when the rectangle has > 32 candidates
     float4* conic;
+    float4* rec;        // GS_TERM_TMIN raster record, 3 float4 per item (RasterRec)
     int2* rect;
+    uint32_t* hitmask;  // bit c = candidate c overlaps (rectangles with <= 32 candidates)
     int32_t* offsets;   // exclusive key offset inside the view
     // scratch
     uint64_t* status;   // [num_views][groups] look-back words
@@ -48,6 +51,7 @@ struct EmitArgs {
     const int64_t* view_total;
     const int64_t* view_base;  // exclusive prefix of view_total
     const int2* rect;
+    const uint32_t* hitmask;  // null: always re-test candidates
     const float2* xy;
     const float4* ell;
     const float* z;
@@ -56,9 +60,17 @@ struct EmitArgs {
     int64_t capacity;
 };
 
+// Raster record of one (view, Gaussian) for GS_TERM_TMIN, written by the
+// frame kernel: the exponent of the splat's density at an offset (dx, dy)
+// is p = A dx^2 + B dx dy + C dy^2 (the conic scaled by -log2(e)/2, so
+// density = exp2(p)), and the cull extents bound the ellipse where
+// opacity * density = kCullAlpha.
+//   r0 = (x, y, A, B)   r1 = (C, opacity, red, green)   r2 = (blue, ext_x, ext_y, 0)
+constexpr float kCullAlpha = 3.814697265625e-06f;  // 2^-18
+
 // Onesweep LSD radix sort of (uint64 key, int32 value) pairs.
-constexpr int kSortThreads = 256;
-constexpr int kSortIpt = 16;
+constexpr int kSortThreads = 512;
+constexpr int kSortIpt = 8;
 constexpr int kSortTile = kSortThreads * kSortIpt;
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;
@@ -79,9 +91,10 @@ struct RasterArgs {
     int64_t num_tiles_total;          // sum of the views' tiles
     const int32_t* ranges;            // [2 * num_tiles_total]
     const int32_t* values;
-    const float2* xy;                 // indexed by value
+    const float2* xy;                 // indexed by value (reference-mode kernel)
     const float4* conic;
     const float4* color;
+    const float4* rec;                // 3 float4 per value (record kernel); null: use xy/conic/color
     float t_min;
     unsigned long long* tile_counter; // persistent variant only
 };

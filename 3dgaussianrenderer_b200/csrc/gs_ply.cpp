@@ -112,7 +112,10 @@ Layout layout_of(const PlyHeader& h)
     return L;
 }
 
-inline float sigmoidf(float x) { return 1.0f / (1.0f + std::exp(-x)); }
+// sigmoid (ply_parser.cpp:10-13) calls the unqualified C exp on a float,
+// which is the double-precision exp: the expression is evaluated in double
+// and rounded to float once, on return.
+inline float sigmoidf(float x) { return (float)(1.0 / (1.0 + std::exp((double)(-x)))); }
 
 inline float clamp01(float v) { return std::min(std::max(v, 0.0f), 1.0f); }
 

@@ -90,11 +90,15 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
     return mhi & ~mlo;
 }
 
-__device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v)
+// Returns this lane's number of overlapping tiles; for rectangles of at
+// most 32 candidates also the hit mask (bit c = candidate c overlaps).
+__device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
+                                               uint32_t& mask)
 {
     const int lane = threadIdx.x & 31;
     const WarpCands w = warp_scan_cands(cand);
     int hits = 0;
+    mask = 0u;
     for (int base = 0; base < w.total; base += 32) {
         const int c = base + lane;
         const int o = owner_of(w.incl, c);
@@ -117,7 +121,12 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
             hit = candidate_hit(oe, orr, c - oexcl, v, tile);
         }
         const unsigned bal = __ballot_sync(kFull, hit);
-        hits += __popc(bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32)));
+        const unsigned bits = bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32));
+        if (bits) {
+            hits += __popc(bits);
+            // lane l of this chunk is candidate base + l - excl of its owner
+            if (cand <= 32) mask |= (w.excl >= base) ? (bits >> (w.excl - base)) : (bits << (base - w.excl));
+        }
     }
     return hits;
 }
@@ -187,7 +196,7 @@ __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
 // within-view key offset from that view's look-back chain.  Gaussians that
 // overlap no tile write only their offset.
 template <int DEG>
-__global__ void __launch_bounds__(256) frame_project_kernel(FrameArgs a)
+__global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
 {
     extern __shared__ __align__(128) float s_sh[];  // [3*(DEG+1)^2][256]
     __shared__ __align__(8) uint64_t s_bar;
@@ -244,18 +253,37 @@ __global__ void __launch_bounds__(256) frame_project_kernel(FrameArgs a)
             r = tile_rect(e, v);
             cand = rect_candidates(r);
         }
-        const int hits = warp_count_hits(e, r, cand, v);
+        uint32_t mask;
+        const int hits = warp_count_hits(e, r, cand, v, mask);
         const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, a.epoch,
                                           a.view_total + view, a.err);
         if (valid) {
             a.offsets[o] = (int32_t)off;
             if (hits > 0) {
-                a.color[o] = col;
-                a.xy[o] = make_float2(s.x, s.y);
                 a.z[o] = s.z;
-                a.ell[o] = make_float4(s.cs, s.sn, s.ex, s.ey);
-                a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
                 a.rect[o] = pack_rect(r);
+                a.hitmask[o] = mask;
+                if (cand > 32) a.ell[o] = make_float4(s.cs, s.sn, s.ex, s.ey);
+                if (a.raster_mode == 0 || cand > 32) a.xy[o] = make_float2(s.x, s.y);
+                if (a.raster_mode == 0) {
+                    a.color[o] = col;
+                    a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
+                } else {
+                    a.rec[3 * o + 0] = make_float4(s.x, s.y, -0.72134752f * s.ca, -1.44269504f * s.cb);
+                    float ex, ey;
+                    const float det = s.ca * s.cc - s.cb * s.cb;
+                    if (!(col.w > kCullAlpha)) {
+                        ex = ey = -1e30f;  // contributes nothing anywhere
+                    } else if (!(det > 0.0f) || !(s.ca > 0.0f) || !(s.cc > 0.0f)) {
+                        ex = ey = 1e30f;  // degenerate conic: never culled
+                    } else {
+                        const float qc = 2.0f * logf(col.w / kCullAlpha);
+                        ex = sqrtf(qc * s.cc / det);
+                        ey = sqrtf(qc * s.ca / det);
+                    }
+                    a.rec[3 * o + 1] = make_float4(-0.72134752f * s.cc, col.w, col.x, col.y);
+                    a.rec[3 * o + 2] = make_float4(col.z, ex, ey, 0.0f);
+                }
             }
         }
     }
@@ -280,9 +308,13 @@ __global__ void __launch_bounds__(256) count_stage_kernel(FrameArgs a)
         cand = rect_candidates(r);
         a.rect[i] = pack_rect(r);
     }
-    const int hits = warp_count_hits(e, r, cand, v);
+    uint32_t mask;
+    const int hits = warp_count_hits(e, r, cand, v, mask);
     const int64_t off = chain_offsets(hits, a.status, tile, a.groups, a.epoch, a.view_total, a.err);
-    if (valid) a.offsets[i] = (int32_t)off;
+    if (valid) {
+        a.offsets[i] = (int32_t)off;
+        a.hitmask[i] = mask;
+    }
 }
 
 __global__ void view_base_kernel(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total)
@@ -327,12 +359,32 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
         if (hits > 0) {
             r = unpack_rect(a.rect[gi]);
             cand = rect_candidates(r);
-            const float2 c = a.xy[gi];
-            const float4 el = a.ell[gi];
-            e = {c.x, c.y, el.x, el.y, el.z, el.w};
             depth = a.z[gi];
+            if (cand <= 32 && a.hitmask) {
+                // the counting pass recorded which candidates overlap: expand
+                // the mask in candidate order, no overlap test needed
+                const ViewParams& v = a.views[view];
+                uint32_t m = a.hitmask[gi];
+                int64_t dst = off;
+                while (m) {
+                    const int c = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int gx = r.x + c % r.z, gy = r.y + c / r.z;
+                    if (dst < a.capacity) {
+                        a.keys[dst] = make_key((uint64_t)(v.tile_offset + gy * v.tiles_x + gx), depth);
+                        a.values[dst] = (int32_t)gi;
+                    }
+                    ++dst;
+                }
+                cand = 0;  // done: stays out of the cooperative walk
+            } else {
+                const float2 c = a.xy[gi];
+                const float4 el = a.ell[gi];
+                e = {c.x, c.y, el.x, el.y, el.z, el.w};
+            }
         }
     }
+    // rectangles with more than 32 candidates: the warp walks them together
     if (__ballot_sync(kFull, cand > 0) == 0) return;
     const WarpCands w = warp_scan_cands(cand);
     int running = 0;

@@ -29,8 +29,6 @@
 
 namespace gs {
 
-constexpr float kCullAlpha = 3.814697265625e-06f;  // 2^-18
-
 struct RasterSmem {
     float2* xy;
     float4* con;  // (a, b, c, opacity)
@@ -197,9 +195,118 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
     }
 }
 
+// ---- GS_TERM_TMIN from raster records --------------------------------------
+//
+// The frame pipeline's kernel for the T_min mode.  One CTA per tile (all
+// views' tiles in one grid), but no CTA-wide barrier: each warp walks the
+// tile's sorted list on its own, 32 entries at a time -- lane l loads entry
+// l's record (48 bytes, gathered through L1, shared by the tile's warps),
+// tests its cull extents against the warp's 8x4 pixel block, and the warp
+// blends the survivors in list order, each broadcast from a per-warp
+// shared-memory slot.  A warp stops when all its pixels have T < t_min.
+// Blend per pixel: p = A dx^2 + B dx dy + C dy^2, alpha = opacity * 2^p,
+// w = T alpha, colour += rgb w, T -= w.
+
+__device__ __forceinline__ float ex2_approx(const float x)
+{
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+template <int TW, int TH>
+__global__ void __launch_bounds__(TW * TH) raster_rec_kernel(RasterArgs a)
+{
+    constexpr int NW = TW * TH / 32;
+    constexpr int WX = TW / 8;
+    __shared__ float4 s_slot[NW][3][32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t gtile = blockIdx.x;
+    int vi = 0;
+    if (a.num_views > 1) {
+        int hi = a.num_views - 1;
+        while (vi < hi) {
+            const int mid = (vi + hi + 1) >> 1;
+            if (a.views[mid].tile_offset <= gtile)
+                vi = mid;
+            else
+                hi = mid - 1;
+        }
+    }
+    const ViewParams& v = a.num_views > 1 ? a.views[vi] : a.view0;
+    const int local_tile = (int)(gtile - v.tile_offset);
+    const int first = __ldg(&a.ranges[2 * gtile]);
+    const int last = __ldg(&a.ranges[2 * gtile + 1]);
+    const int tx = local_tile % v.tiles_x, ty = local_tile / v.tiles_x;
+    const int wx0 = tx * TW + (warp % WX) * 8, wy0 = ty * TH + (warp / WX) * 4;
+    const int px = wx0 + (lane & 7), py = wy0 + (lane >> 3);
+    const bool inimg = px < v.width && py < v.height;
+    if (last - first <= 0) {
+        if (a.write_empty && inimg) v.out[(int64_t)py * v.width + px] = make_uchar4(0, 0, 0, 0);
+        return;
+    }
+    const float cx = (float)px * v.texel_x - 1.0f;
+    const float cy = (float)py * v.texel_y - 1.0f;
+    const float bx0 = (float)wx0 * v.texel_x - 1.0f, bx1 = (float)(wx0 + 7) * v.texel_x - 1.0f;
+    const float by0 = (float)wy0 * v.texel_y - 1.0f, by1 = (float)(wy0 + 3) * v.texel_y - 1.0f;
+    float r = 0.0f, g = 0.0f, b = 0.0f, T = 1.0f;
+    bool done = !inimg;
+    const float tmin = a.t_min;
+
+    for (int base = first; base < last; base += 32) {
+        if (__all_sync(kFull, done)) break;
+        const int j = base + lane;
+        bool keep = false;
+        if (j < last) {
+            const int s = __ldg(&a.values[j]);
+            const float4* rp = a.rec + 3 * (int64_t)s;
+            const float4 r0 = __ldg(rp), r2 = __ldg(rp + 2);
+            keep = (r0.x - r2.y <= bx1) && (r0.x + r2.y >= bx0) && (r0.y - r2.z <= by1) && (r0.y + r2.z >= by0);
+            if (keep) {
+                s_slot[warp][0][lane] = r0;
+                s_slot[warp][1][lane] = __ldg(rp + 1);
+                s_slot[warp][2][lane] = r2;
+            }
+        }
+        unsigned m = __ballot_sync(kFull, keep);
+        __syncwarp();  // slot writes visible to the whole warp
+        while (m) {
+            const int k = __ffs(m) - 1;
+            m &= m - 1;
+            const float4 q0 = s_slot[warp][0][k];
+            const float4 q1 = s_slot[warp][1][k];
+            const float qb = s_slot[warp][2][k].x;
+            if (!done) {
+                const float dx = cx - q0.x, dy = cy - q0.y;
+                const float p = fmaf(fmaf(q0.z, dx, q0.w * dy), dx, q1.x * dy * dy);
+                const float alpha = q1.y * ex2_approx(p);
+                const float w = T * alpha;
+                r = fmaf(q1.z, w, r);
+                g = fmaf(q1.w, w, g);
+                b = fmaf(qb, w, b);
+                T -= w;
+                done = T < tmin;
+            }
+        }
+        __syncwarp();  // slots are rewritten by the next chunk
+    }
+    if (inimg) {
+        uchar4 qc;
+        qc.x = r * 255;
+        qc.y = g * 255;
+        qc.z = b * 255;
+        qc.w = 255;
+        v.out[(int64_t)py * v.width + px] = qc;
+    }
+}
+
 template <int TW, int TH>
 static void launch_shape(const RasterArgs& a, int termination, bool persistent, int num_sms, cudaStream_t st)
 {
+    if (a.rec && termination == 1) {
+        if (a.num_tiles_total > 0) raster_rec_kernel<TW, TH><<<(unsigned)a.num_tiles_total, TW * TH, 0, st>>>(a);
+        return;
+    }
     if (persistent) {
         int per_sm = 0;
         if (termination == 0)

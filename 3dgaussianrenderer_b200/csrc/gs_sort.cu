@@ -19,23 +19,6 @@ namespace gs {
 
 namespace {
 
-__device__ __forceinline__ int64_t block_excl_scan256(const int64_t v, int64_t* s_tmp)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    int64_t incl = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const int64_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-    }
-    if (lane == 31) s_tmp[warp] = incl;
-    __syncthreads();
-    int64_t prefix = 0;
-    for (int w = 0; w < warp; ++w) prefix += s_tmp[w];
-    __syncthreads();
-    return prefix + incl - v;
-}
-
 __device__ __forceinline__ int64_t item_count(const int64_t host_n, const int64_t* dev_n)
 {
     return dev_n ? *dev_n : host_n;
@@ -83,17 +66,39 @@ struct SortPassArgs {
 };
 
 constexpr int kSortSmemBytes = kSortTile * (8 + 4);  // keys + values of one tile
+constexpr int kSortWarps = kSortThreads / 32;
+static_assert(kSortWarps * kRadix * 4 <= kSortSmemBytes, "warp histograms alias the tile buffer");
+static_assert(kSortThreads >= kRadix, "one thread per digit");
 
-__global__ void __launch_bounds__(kSortThreads) onesweep_kernel(SortPassArgs a)
+// Exclusive scan over the block of one value per thread (threads past the
+// digits pass 0).  Every thread of the block must call it.
+__device__ __forceinline__ int64_t block_excl_scan(const int64_t v, int64_t* s_tmp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_tmp[warp] = incl;
+    __syncthreads();
+    int64_t prefix = 0;
+    for (int w = 0; w < warp; ++w) prefix += s_tmp[w];
+    __syncthreads();
+    return prefix + incl - v;
+}
+
+__global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(SortPassArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem);                 // [8][256] while ranking
+    uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem);                 // [warps][256] while ranking
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);                  // [kSortTile] while scattering
     int32_t* s_vals = reinterpret_cast<int32_t*>(smem + kSortTile * 8);    // [kSortTile]
     __shared__ int64_t s_gstart[kRadix];
     __shared__ int64_t s_dstart[kRadix];
     __shared__ int32_t s_bexcl[kRadix];
-    __shared__ int64_t s_scan[8];
+    __shared__ int64_t s_scan[kSortWarps];
     __shared__ int64_t s_tile;
 
     const int64_t n = item_count(a.host_n, a.dev_n);
@@ -104,12 +109,18 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(SortPassArgs a)
     if (tile >= num_tiles) return;
 
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool digit_thread = threadIdx.x < kRadix;
     const int64_t base = tile * kSortTile;
     const int valid = (int)min((int64_t)kSortTile, n - base);
 
     // global start of every digit (exclusive scan of this pass's histogram)
-    s_dstart[threadIdx.x] = block_excl_scan256((int64_t)a.hist[threadIdx.x], s_scan);
+    {
+        const int64_t ds = block_excl_scan(digit_thread ? (int64_t)a.hist[threadIdx.x] : 0, s_scan);
+        if (digit_thread) s_dstart[threadIdx.x] = ds;
+    }
 
+    // warp w owns items [w * 32 * IPT, (w + 1) * 32 * IPT) of the tile, lane
+    // l holds items l, l + 32, ... of that range (coalesced loads)
     uint64_t key[kSortIpt];
     int32_t val[kSortIpt];
     int rank[kSortIpt];
@@ -152,16 +163,19 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(SortPassArgs a)
     __syncthreads();
 
     // per digit: warp offsets, block offsets, look-back across tiles
-    {
+    int run = 0;
+    if (digit_thread) {
         const int d = threadIdx.x;
-        int run = 0;
 #pragma unroll
-        for (int w = 0; w < 8; ++w) {
+        for (int w = 0; w < kSortWarps; ++w) {
             const uint32_t c = s_whist[w * kRadix + d];
             s_whist[w * kRadix + d] = (uint32_t)run;
             run += (int)c;
         }
-        const int64_t bex = block_excl_scan256((int64_t)run, s_scan);
+    }
+    const int64_t bex = block_excl_scan((int64_t)run, s_scan);
+    if (digit_thread) {
+        const int d = threadIdx.x;
         s_bexcl[d] = (int32_t)bex;
         uint64_t* st = a.status + tile * kRadix + d;
         uint64_t excl = 0;
@@ -176,17 +190,16 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_kernel(SortPassArgs a)
     }
     __syncthreads();
 
-    int pos[kSortIpt];
 #pragma unroll
     for (int i = 0; i < kSortIpt; ++i) {
         const unsigned d = (unsigned)(key[i] >> a.shift) & 0xFFu;
-        pos[i] = s_bexcl[d] + (int)s_whist[warp * kRadix + d] + rank[i];
+        rank[i] += s_bexcl[d] + (int)s_whist[warp * kRadix + d];  // position in the tile
     }
     __syncthreads();
 #pragma unroll
     for (int i = 0; i < kSortIpt; ++i) {
-        s_keys[pos[i]] = key[i];
-        s_vals[pos[i]] = val[i];
+        s_keys[rank[i]] = key[i];
+        s_vals[rank[i]] = val[i];
     }
     __syncthreads();
 #pragma unroll

@@ -107,6 +107,66 @@ def cpu_baseline(gs, sc, cams, sample_views=1, threads=None):
                       f"(SH3 + project + build + sort + raster) of the 3M scene, {dt:.1f} s"}
 
 
+SERVE_SCENES = [200_000, 500_000, 1_000_000, 1_000_000, 2_000_000, 2_000_000, 3_000_000, 4_000_000]
+SERVE_RES = [(1280, 720), (1920, 1080), (2560, 1440)]
+
+
+def run_serving(gs, rank, rate=500.0, duration_s=3.0, budget_gb=150, max_batch=16, workers=2):
+    """Serving workload: 8 resident scenes, Poisson request stream at `rate`
+    req/s (scene uniform, pose uniform on a radius-12 sphere, resolution
+    uniform over 720p/1080p/1440p), admitted against a device-memory budget.
+    Latency = submit -> image in host memory."""
+    srv = gs.Server(0, budget_bytes=budget_gb << 30, max_batch_views=max_batch, num_workers=workers)
+    ids = []
+    for k, n in enumerate(SERVE_SCENES):
+        sc = gs.scenes.cluster_scene(n, 256, 10.0, seed=500 + 17 * rank + k)
+        ids.append(srv.add_scene(sc["pos4"], sc["sr4"], gs.scenes.grouped_sh(sc["sh"]), 3))
+        del sc
+    rng = np.random.default_rng(77 + rank)
+    ring = 64
+    bufs = [np.empty(2560 * 1440 * 4, np.uint8) for _ in range(ring)]
+    inflight = [None] * ring
+
+    def make_request():
+        s = ids[int(rng.integers(0, len(ids)))]
+        W, H = SERVE_RES[int(rng.integers(0, len(SERVE_RES)))]
+        cam = gs.look_at(gs.scenes.sphere_pose(rng, 12.0), (0, 0, 0), (0, 1, 0), 50.0, W, H, 0.1, 100.0)
+        return s, cam
+
+    # warm-up: every scene and resolution once
+    for s in ids:
+        for (W, H) in SERVE_RES:
+            cam = gs.look_at((0.0, 1.0, 12.0), (0, 0, 0), (0, 1, 0), 50.0, W, H, 0.1, 100.0)
+            srv.wait(srv.submit(s, cam, bufs[0]))
+    srv.reset_stats()
+    t0 = time.perf_counter()
+    t_next = t0
+    slot = 0
+    count = 0
+    while True:
+        t_next += rng.exponential(1.0 / rate)
+        if t_next - t0 > duration_s:
+            break
+        s, cam = make_request()
+        if inflight[slot] is not None:
+            srv.wait(inflight[slot])
+        delay = t_next - time.perf_counter()
+        if delay > 0:
+            time.sleep(delay)
+        inflight[slot] = srv.submit(s, cam, bufs[slot])
+        slot = (slot + 1) % ring
+        count += 1
+    for r in inflight:
+        if r is not None:
+            srv.wait(r)
+    st = srv.stats()
+    srv.close()
+    return {"views_per_s": st["views_per_s"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_ms": st["mean_ms"], "requests": count, "rate_req_s": rate, "max_batch": st["max_batch"],
+            "batches": st["batches_done"], "budget_gb": budget_gb, "workers": workers,
+            "scenes_m": [n / 1e6 for n in SERVE_SCENES]}
+
+
 def run_reference(args, rank, world):
     import torch.distributed as dist
     if rank != 0:
@@ -225,6 +285,15 @@ def run_ours(args, rank, world, local_rank):
         torch.cuda.synchronize()
         plain_value = plain_views / (g0.elapsed_time(g1) / 1e3)
 
+    served = None
+    if not args.no_serve:
+        # release this leg's frame buffers first: the server has its own
+        del outs
+        ctx.close()
+        scene.close()
+        torch.cuda.empty_cache()
+        served = run_serving(gs, rank)
+
     if rank != 0:
         return
     hbm, peak_kind = peaks()
@@ -256,6 +325,8 @@ def run_ours(args, rank, world, local_rank):
         "e2e": {"value": e2e_value, "unit": "views/s", "h2d_bytes_per_step": VIEWS * 200,
                 "d2h_bytes_per_step": total_bytes},
         "plain_views_per_s": plain_value,
+        "batched_over_plain": (value / world / plain_value) if plain_value else None,
+        "served": served,
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -273,6 +344,7 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-plain", action="store_true", help="skip the single-view leg (profiling runs)")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg (profiling runs)")
     ap.add_argument("--views", type=int, default=VIEWS,
                     help="views per batched frame (64 = the workload; fewer only for small profiling cases)")
     args = ap.parse_args()

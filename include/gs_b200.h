@@ -172,6 +172,40 @@ GS_API int gs_stage_ranges(int64_t num_keys, const uint64_t* d_keys, int64_t num
 GS_API int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_t* d_ranges, const int32_t* d_values,
                     const float* d_xy, const float* d_conic, const float* d_color, uint8_t* d_rgba, void* stream);
 
+/* ---- serving: resident scenes, continuous batching ---------------------- */
+/* No counterpart in the reference (a single-scene desktop viewer); this is
+ * the serving loop built on the batched frame.  Scenes stay resident; view
+ * requests from any thread are grouped per scene into batched frames as
+ * workers free up (each worker: its own context and stream, so batches
+ * overlap on the device), admitted against a device-memory budget. */
+typedef struct gs_server gs_server;
+typedef struct gs_server_cfg {
+    int64_t budget_bytes;     /* scenes + frame buffers must fit (150 GiB default) */
+    int32_t max_batch_views;  /* views per batched frame */
+    int32_t num_workers;      /* batches in flight */
+    gs_render_cfg render;
+} gs_server_cfg;
+typedef struct gs_server_stats {
+    int64_t views_done, batches_done, max_batch;
+    double p50_ms, p99_ms, mean_ms; /* submit -> image in the host buffer */
+    double views_per_s;             /* views done / (last completion - first submit) */
+    int64_t resident_bytes, frame_bytes, pending;
+} gs_server_stats;
+
+GS_API void gs_server_default_cfg(gs_server_cfg* cfg);
+GS_API int gs_server_create(int device, const gs_server_cfg* cfg, gs_server** out);
+GS_API int gs_server_destroy(gs_server* server);
+/* GS_ERR_CAPACITY when the scene does not fit the budget. */
+GS_API int gs_server_add_scene(gs_server* server, int64_t n, const float* h_position, const float* h_scale_rotation,
+                               const float* h_color, const float* h_sh, int32_t sh_degree, int32_t* out_scene_id);
+/* Non-blocking; h_rgba (4*W*H bytes, host) is written before the request completes. */
+GS_API int gs_server_submit(gs_server* server, int32_t scene_id, const gs_camera* cam, uint8_t* h_rgba,
+                            int64_t* out_request_id);
+/* Waits up to timeout_ms; returns the request's status (GS_ERR_DEVICE_TIMEOUT if not done). */
+GS_API int gs_server_wait(gs_server* server, int64_t request_id, double timeout_ms, double* out_latency_ms);
+GS_API int gs_server_get_stats(gs_server* server, gs_server_stats* out);
+GS_API int gs_server_reset_stats(gs_server* server);
+
 /* ---- model ingest (parsePly / savePly, core/ply_parser.cpp:15-393) ------ */
 /* Binary little-endian PLY with float properties named as the INRIA 3DGS
  * exporter writes them (x y z rot_0..3 scale_0..2 f_dc_0..2 f_rest_* opacity).

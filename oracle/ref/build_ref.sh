@@ -50,3 +50,12 @@ nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -lineinfo \
   -diag-suppress 20012,20014,20011,20013,177,550,2361,3012,1444 \
   "$TMP/ref_harness.cu" -o "$OUT/libgsref.so"
 echo "build_ref: wrote $OUT/libgsref.so"
+
+# parsePly compiles as it lies (plain C++; glm and CUDA's vector_types.h);
+# -ffp-contract=off keeps its float arithmetic uncontracted, as MSVC's
+# default /fp:precise does.
+g++ -std=c++20 -O2 -fPIC -shared -ffp-contract=off \
+  -I"$REF/core" -I"$REF/external/glm" -I/usr/local/cuda/include \
+  -include cassert -include limits \
+  "$REPO/oracle/ref/ply_ref_harness.cpp" "$REF/core/ply_parser.cpp" -o "$OUT/libplyref.so"
+echo "build_ref: wrote $OUT/libplyref.so"
