@@ -426,6 +426,7 @@ class gs_server_cfg(ctypes.Structure):
         ("max_batch_views", ctypes.c_int32),
         ("num_workers", ctypes.c_int32),
         ("render", gs_render_cfg),
+        ("batch_target_ms", ctypes.c_double),
     ]
 
 
@@ -466,12 +467,14 @@ class Server:
     from any thread, batched frames formed as workers free up."""
 
     def __init__(self, device: int = 0, budget_bytes: int = 150 << 30, max_batch_views: int = 16,
-                 num_workers: int = 2, cfg: RenderConfig | None = None):
+                 num_workers: int = 2, cfg: RenderConfig | None = None, batch_target_ms: float | None = None):
         c = gs_server_cfg()
         lib.gs_server_default_cfg(ctypes.byref(c))
         c.budget_bytes = budget_bytes
         c.max_batch_views = max_batch_views
         c.num_workers = num_workers
+        if batch_target_ms is not None:
+            c.batch_target_ms = batch_target_ms
         if cfg is not None:
             c.render = cfg.c()
         h = _P()

@@ -51,6 +51,7 @@ struct SceneEntry {
     int64_t n = 0;
     int64_t bytes = 0;
     double keys_per_gaussian = 2.0;  // refined from every rendered batch
+    double ms_per_mpixel = 0.0;      // batch time per million output pixels, refined likewise
 };
 
 struct Worker {
@@ -59,8 +60,8 @@ struct Worker {
     std::thread th;
     std::vector<Request> batch;
     bool has_batch = false;
-    uint8_t* staging = nullptr;  // pinned image staging
-    size_t staging_bytes = 0;
+    uint8_t* images = nullptr;  // device images of the current batch
+    size_t image_bytes = 0;
 };
 
 }  // namespace
@@ -110,6 +111,7 @@ void worker_loop(gs_server* S, Worker* w)
             if (!w->has_batch && S->stop) return;
             batch.swap(w->batch);
         }
+        const Clock::time_point t0 = Clock::now();
         const int32_t sid = batch.front().scene;
         gs_scene* scene = nullptr;
         {
@@ -117,34 +119,43 @@ void worker_loop(gs_server* S, Worker* w)
             scene = S->scenes[sid].scene;
         }
         std::vector<gs_camera> cams;
+        std::vector<size_t> offs;
         size_t total = 0;
         for (const Request& r : batch) {
             cams.push_back(r.cam);
+            offs.push_back(total);
             total += 4 * (size_t)r.cam.width * r.cam.height;
         }
         int status = GS_OK;
-        if (total > w->staging_bytes) {
-            if (w->staging) cudaFreeHost(w->staging);
-            w->staging = nullptr;
-            w->staging_bytes = 0;
-            if (cudaMallocHost(&w->staging, total) == cudaSuccess)
-                w->staging_bytes = total;
+        if (total > w->image_bytes) {
+            // grow-only, with headroom, so steady state never allocates
+            if (w->images) cudaFree(w->images);
+            w->images = nullptr;
+            w->image_bytes = 0;
+            const size_t want = total + total / 2;
+            if (cudaMalloc(&w->images, want) == cudaSuccess)
+                w->image_bytes = want;
             else
                 status = GS_ERR_OOM;
         }
         gs_stats st{};
-        if (status == GS_OK)
-            status = gs_render_batch_host(w->ctx, scene, cams.data(), (int32_t)cams.size(), &S->cfg.render, w->staging,
-                                          &st, w->stream);
-        size_t off = 0;
-        const Clock::time_point now0 = Clock::now();
-        for (const Request& r : batch) {
-            const size_t b = 4 * (size_t)r.cam.width * r.cam.height;
-            if (status == GS_OK) std::memcpy(r.out, w->staging + off, b);
-            off += b;
+        if (status == GS_OK) {
+            std::vector<uint8_t*> outs;
+            for (size_t o : offs) outs.push_back(w->images + o);
+            status = gs_render_batch(w->ctx, scene, cams.data(), (int32_t)cams.size(), &S->cfg.render, outs.data(),
+                                     &st, w->stream);
+        }
+        if (status == GS_OK) {
+            // every view straight into its request's host buffer
+            for (size_t k = 0; k < batch.size(); ++k) {
+                const size_t b = 4 * (size_t)batch[k].cam.width * batch[k].cam.height;
+                if (cudaMemcpyAsync(batch[k].out, w->images + offs[k], b, cudaMemcpyDeviceToHost, w->stream) !=
+                    cudaSuccess)
+                    status = GS_ERR_CUDA;
+            }
+            if (cudaStreamSynchronize(w->stream) != cudaSuccess) status = GS_ERR_CUDA;
         }
         const Clock::time_point now = Clock::now();
-        (void)now0;
         {
             std::lock_guard<std::mutex> lk(S->mu);
             for (const Request& r : batch) {
@@ -157,6 +168,12 @@ void worker_loop(gs_server* S, Worker* w)
                 if (se.n > 0 && st.num_keys > 0)
                     se.keys_per_gaussian = 0.5 * se.keys_per_gaussian +
                                            0.5 * (double)st.num_keys / ((double)se.n * (double)batch.size());
+                const double mp = (double)total / 4.0 / 1e6;
+                const double batch_ms = std::chrono::duration<double, std::milli>(now - t0).count();
+                if (mp > 0) {
+                    const double x = batch_ms / mp;
+                    se.ms_per_mpixel = se.ms_per_mpixel > 0 ? 0.7 * se.ms_per_mpixel + 0.3 * x : x;
+                }
                 S->views_done += (int64_t)batch.size();
                 S->batches_done += 1;
                 S->max_batch_seen = std::max<int64_t>(S->max_batch_seen, (int64_t)batch.size());
@@ -212,6 +229,16 @@ void scheduler_loop(gs_server* S)
                 batch.pop_back();
                 break;
             }
+            // keep the batch within the latency target, from the scene's
+            // measured cost per output pixel
+            if (batch.size() > 1 && se.ms_per_mpixel > 0 && S->cfg.batch_target_ms > 0) {
+                double mp = 0;
+                for (const Request& q : batch) mp += (double)q.cam.width * q.cam.height / 1e6;
+                if (mp * se.ms_per_mpixel > S->cfg.batch_target_ms) {
+                    batch.pop_back();
+                    break;
+                }
+            }
             it = S->pending.erase(it);
         }
         if (batch.empty()) {
@@ -235,6 +262,7 @@ GS_API void gs_server_default_cfg(gs_server_cfg* cfg)
     cfg->budget_bytes = 150ll << 30;
     cfg->max_batch_views = 16;
     cfg->num_workers = 2;
+    cfg->batch_target_ms = 8.0;
     gs_default_cfg(&cfg->render);
 }
 
@@ -289,7 +317,7 @@ GS_API int gs_server_destroy(gs_server* S)
     for (auto& w : S->workers) {
         gs_ctx_destroy(w->ctx);
         cudaStreamDestroy(w->stream);
-        if (w->staging) cudaFreeHost(w->staging);
+        if (w->images) cudaFree(w->images);
     }
     for (auto& kv : S->scenes) gs_scene_destroy(kv.second.scene);
     gs_ctx_destroy(S->owner);

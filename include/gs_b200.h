@@ -184,6 +184,7 @@ typedef struct gs_server_cfg {
     int32_t max_batch_views;  /* views per batched frame */
     int32_t num_workers;      /* batches in flight */
     gs_render_cfg render;
+    double batch_target_ms;   /* a batch stops growing once its estimated time exceeds this (8 ms; 0 = off) */
 } gs_server_cfg;
 typedef struct gs_server_stats {
     int64_t views_done, batches_done, max_batch;
