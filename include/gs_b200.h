@@ -162,6 +162,21 @@ GS_API int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float
 GS_API int gs_stage_sort(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, uint64_t* d_keys, int32_t* d_values,
                   uint64_t* d_keys_alt, int32_t* d_values_alt, int32_t* out_selector, void* stream);
 
+/* No counterpart in the reference.  The same sort as gs_stage_sort, for
+ * callers that must not allocate device memory (an application that hands
+ * out all device memory from its own pool, or a frame loop that cannot afford
+ * the device-wide synchronisation of cudaMalloc/cudaFree): its scratch is a
+ * fixed array inside the library (about 2 MiB on every GPU that loads it) and
+ * the call allocates nothing.  At most gs_stage_sort_noalloc_max_keys()
+ * (4,194,304) keys; more returns GS_ERR_CAPACITY.  All calls share the array:
+ * calls that overlap on the GPU race, so serialise them.  The first call on
+ * a device resolves the array's address; make it before any stream capture.
+ * Synchronises `stream` before returning. */
+GS_API int gs_stage_sort_noalloc(int64_t num_keys, int32_t key_bits, uint64_t* d_keys, int32_t* d_values,
+                                 uint64_t* d_keys_alt, int32_t* d_values_alt, int32_t* out_selector, void* stream);
+GS_API int64_t gs_stage_sort_noalloc_max_keys(void);
+GS_API const char* gs_stage_sort_noalloc_error(void);
+
 /* evaluateTileRange (gaussian_render.cu:634-677).  Fills all 2*num_tiles
  * entries: tiles without keys get (-1, -1) as after the reference's
  * 0xFF clear (main.cpp:365). */
