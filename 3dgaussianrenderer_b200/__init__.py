@@ -67,7 +67,8 @@ class gs_render_cfg(ctypes.Structure):
         ("t_min", ctypes.c_float),
         ("tile_w", ctypes.c_int32),
         ("tile_h", ctypes.c_int32),
-        ("raster_batch", ctypes.c_int32),
+        ("sort_variant", ctypes.c_int32),
+        ("views_per_block", ctypes.c_int32),
     ]
 
 
@@ -257,7 +258,8 @@ class RenderConfig:
     t_min: float = 1e-4
     tile_w: int = 16
     tile_h: int = 16
-    raster_batch: int = 0
+    sort_variant: int = 0
+    views_per_block: int = 0
 
     @staticmethod
     def reference() -> "RenderConfig":
@@ -265,7 +267,7 @@ class RenderConfig:
 
     def c(self) -> gs_render_cfg:
         return gs_render_cfg(self.sh_max_degree, self.termination, self.t_min, self.tile_w, self.tile_h,
-                             self.raster_batch)
+                             self.sort_variant, self.views_per_block)
 
 
 def num_tiles(width: int, height: int, cfg: RenderConfig) -> int:

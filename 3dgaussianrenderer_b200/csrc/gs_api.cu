@@ -158,7 +158,8 @@ bool valid_cfg(const gs_render_cfg& c)
 {
     const bool shape = (c.tile_w == 16 && c.tile_h == 16) || (c.tile_w == 16 && c.tile_h == 8) ||
                        (c.tile_w == 8 && c.tile_h == 8);
-    return shape && c.sh_max_degree >= 0 && c.sh_max_degree <= 3 &&
+    return shape && c.sh_max_degree >= 0 && c.sh_max_degree <= 3 && c.sort_variant >= 0 &&
+           c.sort_variant < kSortVariants && c.views_per_block >= 0 &&
            (c.termination == GS_TERM_REFERENCE || c.termination == GS_TERM_TMIN);
 }
 
@@ -178,7 +179,7 @@ float ms_between(cudaEvent_t a, cudaEvent_t b)
 
 int ensure_sort_scratch(gs_ctx* ctx, int64_t num_items)
 {
-    const int64_t tiles = (num_items + kSortTile - 1) / kSortTile;
+    const int64_t tiles = (num_items + kSortMinTile - 1) / kSortMinTile;
     if (ctx->sort_hist.ensure(sizeof(uint32_t) * kMaxPasses * kRadix) != cudaSuccess) return fail(GS_ERR_OOM, "sort hist");
     const size_t need = sizeof(uint64_t) * (size_t)std::max<int64_t>(tiles, 1) * kRadix;
     if (need > ctx->sort_status.bytes) {
@@ -241,7 +242,7 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     if (items >= (1ll << 31)) return fail(GS_ERR_INVALID, "views x Gaussians exceeds 2^31");
     const int64_t groups = (n + 255) / 256;
     // views per block: the SH chunk of a group is read once per block
-    const int vpb = std::min(num_views, 8);
+    const int vpb = std::min(num_views, cfg.views_per_block > 0 ? cfg.views_per_block : 16);
     const int64_t blocks = groups * ((num_views + vpb - 1) / vpb);
     const int64_t chains = groups * num_views;
 
@@ -269,7 +270,7 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     GS_CUDA(cudaEventRecord(ctx->ev[0], st));
 
     // 1. SH + projection + exact tile counts + key offsets
-    FrameArgs fa;
+    FrameArgs fa{};
     fa.n = n;
     fa.groups = groups;
     fa.num_views = num_views;
@@ -353,7 +354,8 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     if (K > 0) {
         const uint32_t ep = take_epochs(ctx->epoch_sort, (uint32_t)sort_passes(key_bits), ctx->sort_status, st);
         passes = launch_sort(ctx->keys0.as<uint64_t>(), ctx->vals0.as<int32_t>(), ctx->keys1.as<uint64_t>(),
-                             ctx->vals1.as<int32_t>(), K, nullptr, key_bits, ss, ep, ctx->num_sms, st);
+                             ctx->vals1.as<int32_t>(), K, nullptr, key_bits, ss, ep, ctx->num_sms, st,
+                             cfg.sort_variant);
     }
     GS_CUDA(cudaGetLastError());
     const uint64_t* skeys = (passes % 2) ? ctx->keys1.as<uint64_t>() : ctx->keys0.as<uint64_t>();
@@ -434,7 +436,8 @@ void gs_default_cfg(gs_render_cfg* cfg)
     cfg->t_min = 1e-4f;
     cfg->tile_w = 16;
     cfg->tile_h = 16;
-    cfg->raster_batch = 0;
+    cfg->sort_variant = 0;
+    cfg->views_per_block = 0;
 }
 
 void gs_camera_look_at(gs_camera* cam, const float eye[3], const float target[3], const float up[3], float fovy_rad,

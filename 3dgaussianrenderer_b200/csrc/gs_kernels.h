@@ -17,6 +17,7 @@ struct FrameArgs {
     int32_t num_views;
     int32_t views_per_block;
     uint32_t epoch;     // look-back epoch of this launch
+    const uint32_t* epoch_dev;  // non-null: the epoch is read here (graph replays)
     int64_t num_tiles;  // blocks = ceil(num_views / views_per_block) * groups
     const float4* pos;
     const float4* sr;
@@ -68,10 +69,12 @@ struct EmitArgs {
 //   r0 = (x, y, A, B)   r1 = (C, opacity, red, green)   r2 = (blue, ext_x, ext_y, 0)
 constexpr float kCullAlpha = 3.814697265625e-06f;  // 2^-18
 
-// Onesweep LSD radix sort of (uint64 key, int32 value) pairs.
-constexpr int kSortThreads = 512;
-constexpr int kSortIpt = 8;
-constexpr int kSortTile = kSortThreads * kSortIpt;
+// Onesweep LSD radix sort of (uint64 key, int32 value) pairs.  Tiles of
+// 2048, 4096 or 8192 keys (sort_tile_items(variant)); kSortTile is the
+// default variant's, kSortMinTile sizes the look-back words for all.
+constexpr int kSortTile = 4096;
+constexpr int kSortMinTile = 2048;
+constexpr int kSortVariants = 4;
 constexpr int kRadix = 256;
 constexpr int kMaxPasses = 8;
 
@@ -105,17 +108,23 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
                           float* z, float4* ell, float4* conic, cudaStream_t st);
 void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st);
 void launch_count_stage(const FrameArgs& a, cudaStream_t st);
-// view_base[v] = sum of view_total[u < v]; *total = sum of all.
-void launch_view_base(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total, cudaStream_t st);
+// view_base[v] = sum of view_total[u < v]; *total = sum of all.  With a
+// non-null `sort_n`, also *sort_n = min(total, capacity) and *overflow = 1
+// when the keys do not fit (frames whose key count is not known on the host).
+void launch_view_base(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total, cudaStream_t st,
+                      int64_t capacity = 0, int64_t* sort_n = nullptr, int* overflow = nullptr);
 void launch_emit(const EmitArgs& a, cudaStream_t st);
 
 // Sorts num_items pairs on bits [0, key_bits).  When d_num_items is non-null
 // the item count is read on the device (graph-friendly; num_items is then
-// an upper bound used to size the grids).  Returns the number of passes;
-// the result is in the alternate buffers when that number is odd.
+// an upper bound used to size the grids); likewise a non-null d_epoch
+// replaces `epoch` as the look-back epoch of the first pass.  Returns the
+// number of passes; the result is in the alternate buffers when that number
+// is odd.
 int launch_sort(const uint64_t* keys_in, const int32_t* vals_in, uint64_t* keys_alt, int32_t* vals_alt,
                 int64_t num_items, const int64_t* d_num_items, int key_bits, const SortScratch& s, uint32_t epoch,
-                int num_sms, cudaStream_t st);
+                int num_sms, cudaStream_t st, int variant = 0, const uint32_t* d_epoch = nullptr);
+int sort_tile_items(int variant);
 int sort_passes(int key_bits);
 
 void launch_ranges(const uint64_t* keys, int64_t num_items, const int64_t* d_num_items, int32_t* ranges,

@@ -207,6 +207,7 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
     const bool valid = i < a.n;
     const int v0 = (int)chunk * a.views_per_block;
     const int v1 = min(a.num_views, v0 + a.views_per_block);
+    const uint32_t epoch = a.epoch_dev ? *a.epoch_dev : a.epoch;
     constexpr int NCOEF = DEG >= 0 ? 3 * (DEG + 1) * (DEG + 1) : 0;
 
     if (DEG >= 0) {
@@ -255,7 +256,7 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
         }
         uint32_t mask;
         const int hits = warp_count_hits(e, r, cand, v, mask);
-        const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, a.epoch,
+        const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, epoch,
                                           a.view_total + view, a.err);
         if (valid) {
             a.offsets[o] = (int32_t)off;
@@ -317,7 +318,8 @@ __global__ void __launch_bounds__(256) count_stage_kernel(FrameArgs a)
     }
 }
 
-__global__ void view_base_kernel(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total)
+__global__ void view_base_kernel(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total,
+                                 int64_t capacity, int64_t* sort_n, int* overflow)
 {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         int64_t run = 0;
@@ -326,6 +328,10 @@ __global__ void view_base_kernel(const int64_t* view_total, int num_views, int64
             run += view_total[v];
         }
         *total = run;
+        if (sort_n) {
+            *sort_n = run < capacity ? run : capacity;
+            *overflow = run > capacity ? 1 : 0;
+        }
     }
 }
 
@@ -482,9 +488,10 @@ void launch_count_stage(const FrameArgs& a, cudaStream_t st)
     count_stage_kernel<<<grid, 256, 0, st>>>(a);
 }
 
-void launch_view_base(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total, cudaStream_t st)
+void launch_view_base(const int64_t* view_total, int num_views, int64_t* view_base, int64_t* total, cudaStream_t st,
+                      int64_t capacity, int64_t* sort_n, int* overflow)
 {
-    view_base_kernel<<<1, 32, 0, st>>>(view_total, num_views, view_base, total);
+    view_base_kernel<<<1, 32, 0, st>>>(view_total, num_views, view_base, total, capacity, sort_n, overflow);
 }
 
 void launch_emit(const EmitArgs& a, cudaStream_t st)

@@ -59,16 +59,14 @@ struct SortPassArgs {
     const int64_t* dev_n;
     int shift;
     uint32_t epoch;
+    const uint32_t* epoch_dev;  // non-null: epoch = *epoch_dev + pass
+    int pass;
     const uint32_t* hist;  // this pass's 256 bins
     uint64_t* status;
     unsigned long long* counter;
     int* err;
 };
 
-constexpr int kSortSmemBytes = kSortTile * (8 + 4);  // keys + values of one tile
-constexpr int kSortWarps = kSortThreads / 32;
-static_assert(kSortWarps * kRadix * 4 <= kSortSmemBytes, "warp histograms alias the tile buffer");
-static_assert(kSortThreads >= kRadix, "one thread per digit");
 
 // Exclusive scan over the block of one value per thread (threads past the
 // digits pass 0).  Every thread of the block must call it.
@@ -89,8 +87,16 @@ __device__ __forceinline__ int64_t block_excl_scan(const int64_t v, int64_t* s_t
     return prefix + incl - v;
 }
 
-__global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(SortPassArgs a)
+// One onesweep pass over THREADS x IPT-key tiles (MINB blocks per SM).
+template <int THREADS, int IPT, int MINB>
+__global__ void __launch_bounds__(THREADS, MINB) onesweep_kernel(SortPassArgs a)
 {
+    constexpr int kSortTile = THREADS * IPT;
+    constexpr int kSortIpt = IPT;
+    constexpr int kSortThreads = THREADS;
+    constexpr int kSortWarps = THREADS / 32;
+    static_assert(kSortWarps * kRadix * 4 <= kSortTile * 12, "warp histograms alias the tile buffer");
+    static_assert(THREADS >= kRadix, "one thread per digit");
     extern __shared__ __align__(16) unsigned char smem[];
     uint32_t* s_whist = reinterpret_cast<uint32_t*>(smem);                 // [warps][256] while ranking
     uint64_t* s_keys = reinterpret_cast<uint64_t*>(smem);                  // [kSortTile] while scattering
@@ -102,6 +108,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(SortPassArgs 
     __shared__ int64_t s_tile;
 
     const int64_t n = item_count(a.host_n, a.dev_n);
+    const uint32_t epoch = a.epoch_dev ? *a.epoch_dev + (uint32_t)a.pass : a.epoch;
     const int64_t num_tiles = (n + kSortTile - 1) / kSortTile;
     if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(a.counter, 1ull);
     __syncthreads();
@@ -180,11 +187,11 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(SortPassArgs 
         uint64_t* st = a.status + tile * kRadix + d;
         uint64_t excl = 0;
         if (tile == 0) {
-            store_status(st, status_word(kFlagP, a.epoch, (uint64_t)run));
+            store_status(st, status_word(kFlagP, epoch, (uint64_t)run));
         } else {
-            store_status(st, status_word(kFlagA, a.epoch, (uint64_t)run));
-            excl = look_back(a.status + d, tile, kRadix, a.epoch, a.err, kErrTimeout);
-            store_status(st, status_word(kFlagP, a.epoch, excl + (uint64_t)run));
+            store_status(st, status_word(kFlagA, epoch, (uint64_t)run));
+            excl = look_back(a.status + d, tile, kRadix, epoch, a.err, kErrTimeout);
+            store_status(st, status_word(kFlagP, epoch, excl + (uint64_t)run));
         }
         s_gstart[d] = s_dstart[d] + (int64_t)excl;
     }
@@ -217,22 +224,54 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_kernel(SortPassArgs 
 
 int sort_passes(int key_bits) { return (key_bits + 7) / 8; }
 
+template <int THREADS, int IPT, int MINB>
+static void launch_pass_t(const SortPassArgs& a, int64_t num_items, cudaStream_t st)
+{
+    constexpr int tile = THREADS * IPT;
+    constexpr int smem = tile * 12;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(onesweep_kernel<THREADS, IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    const int64_t tiles = (num_items + tile - 1) / tile;
+    onesweep_kernel<THREADS, IPT, MINB><<<(unsigned)tiles, THREADS, smem, st>>>(a);
+}
+
+// Tile shapes of the onesweep pass (the autotuner picks one per workload).
+static void launch_pass(const SortPassArgs& a, int64_t num_items, int variant, cudaStream_t st)
+{
+    switch (variant) {
+        case 1: launch_pass_t<256, 8, 4>(a, num_items, st); break;    // 2048 keys, 4 blocks/SM
+        case 2: launch_pass_t<256, 16, 2>(a, num_items, st); break;   // 4096 keys, 16 keys/thread
+        case 3: launch_pass_t<512, 16, 1>(a, num_items, st); break;   // 8192 keys
+        default: launch_pass_t<512, 8, 2>(a, num_items, st); break;   // 4096 keys, 2 blocks/SM
+    }
+}
+
+int sort_tile_items(int variant)
+{
+    switch (variant) {
+        case 1: return 2048;
+        case 3: return 8192;
+        default: return 4096;
+    }
+}
+
 int launch_sort(const uint64_t* keys_in, const int32_t* vals_in, uint64_t* keys_alt, int32_t* vals_alt,
                 int64_t num_items, const int64_t* d_num_items, int key_bits, const SortScratch& s, uint32_t epoch,
-                int num_sms, cudaStream_t st)
+                int num_sms, cudaStream_t st, int variant, const uint32_t* d_epoch)
 {
     const int passes = sort_passes(key_bits);
     if (num_items <= 0 || passes == 0) return 0;
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(onesweep_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kSortSmemBytes);
         cudaFuncSetAttribute(sort_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              8 * kMaxPasses * kRadix * 4);
         attr_set = true;
     }
     cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, st);
     cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long) * kMaxPasses, st);
-    const int64_t tiles = (num_items + kSortTile - 1) / kSortTile;
     const int hist_blocks = (int)std::min<int64_t>((int64_t)num_sms * 4, std::max<int64_t>(1, (num_items + 4095) / 4096));
     sort_hist_kernel<<<hist_blocks, 256, 8 * passes * kRadix * 4, st>>>(keys_in, num_items, d_num_items, passes,
                                                                          s.hist);
@@ -249,11 +288,13 @@ int launch_sort(const uint64_t* keys_in, const int32_t* vals_in, uint64_t* keys_
         a.dev_n = d_num_items;
         a.shift = 8 * p;
         a.epoch = epoch + (uint32_t)p;
+        a.epoch_dev = d_epoch;
+        a.pass = p;
         a.hist = s.hist + p * kRadix;
         a.status = s.status;
         a.counter = s.counters + p;
         a.err = s.err;
-        onesweep_kernel<<<(unsigned)tiles, kSortThreads, kSortSmemBytes, st>>>(a);
+        launch_pass(a, num_items, variant, st);
     }
     return passes;
 }

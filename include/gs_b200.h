@@ -70,7 +70,8 @@ typedef struct gs_render_cfg {
     int32_t termination;   /* GS_TERM_REFERENCE (T<=0.02 tile-wide every 32 entries) or GS_TERM_TMIN */
     float t_min;           /* per-pixel transmittance floor for GS_TERM_TMIN (1e-4) */
     int32_t tile_w, tile_h;/* 16x16 (reference), 16x8 or 8x8 */
-    int32_t raster_batch;  /* splats staged per shared-memory batch: 32..256 (0 = default) */
+    int32_t sort_variant;  /* onesweep tile shape: 0 = 512x8 keys, 1 = 256x8, 2 = 256x16, 3 = 512x16 */
+    int32_t views_per_block; /* views the fused projection handles per block (0 = 8) */
 } gs_render_cfg;
 
 /* Per-stage device times of one frame, same fields as the reference's
