@@ -38,6 +38,8 @@ GS_ERR_CUDA = 5
 GS_ERR_NO_DEVICE = 6
 GS_TERM_REFERENCE = 0
 GS_TERM_TMIN = 1
+GS_ORDER_BUCKETS = 0
+GS_ORDER_ONESWEEP = 1
 
 
 class GsError(RuntimeError):
@@ -67,8 +69,10 @@ class gs_render_cfg(ctypes.Structure):
         ("t_min", ctypes.c_float),
         ("tile_w", ctypes.c_int32),
         ("tile_h", ctypes.c_int32),
+        ("ordering", ctypes.c_int32),
         ("sort_variant", ctypes.c_int32),
         ("views_per_block", ctypes.c_int32),
+        ("graph", ctypes.c_int32),
     ]
 
 
@@ -83,6 +87,8 @@ class gs_stats(ctypes.Structure):
         ("num_keys", ctypes.c_int64),
         ("num_tiles", ctypes.c_int64),
         ("kernel_launches", ctypes.c_int64),
+        ("graph_replay", ctypes.c_int32),
+        ("attempts", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -258,8 +264,10 @@ class RenderConfig:
     t_min: float = 1e-4
     tile_w: int = 16
     tile_h: int = 16
+    ordering: int = 0  # GS_ORDER_BUCKETS
     sort_variant: int = 0
     views_per_block: int = 0
+    graph: int = 1
 
     @staticmethod
     def reference() -> "RenderConfig":
@@ -267,7 +275,7 @@ class RenderConfig:
 
     def c(self) -> gs_render_cfg:
         return gs_render_cfg(self.sh_max_degree, self.termination, self.t_min, self.tile_w, self.tile_h,
-                             self.sort_variant, self.views_per_block)
+                             self.ordering, self.sort_variant, self.views_per_block, self.graph)
 
 
 def num_tiles(width: int, height: int, cfg: RenderConfig) -> int:

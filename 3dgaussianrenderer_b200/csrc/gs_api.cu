@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <mutex>
 #include <new>
 #include <string>
@@ -80,19 +81,43 @@ struct DevBuf {
     }
 };
 
-// Small per-context device words, cleared with one memset per frame.
+// Small per-context device words, reset at the start of every frame (by a
+// copy of the pinned `h_init`, which also carries the frame's look-back
+// epochs, so a captured frame reads fresh epochs on every replay).
 struct Counters {
     unsigned long long frame_tile;                 // frame kernel block queue
     unsigned long long raster_tile;                // persistent raster queue
     unsigned long long sort_tiles[kMaxPasses];     // onesweep tile queues
+    unsigned long long scan_block;                 // tile scan block queue
+    unsigned long long slots;                      // (view, Gaussian) slots taken by the frame kernel
     int64_t total;                                 // K
+    int64_t sort_n;                                // min(K, key capacity)
     int err;
-    int pad;
+    int overflow;                                  // K > key capacity: the frame must be redone
+    uint32_t epoch_scan, epoch_sort;               // look-back epochs of this frame
 };
+
+// A frame captured into a CUDA graph, or a frame seen once (no `exec` yet):
+// the graph is captured the second time the same key comes along.
+struct FrameGraph {
+    uint64_t scene_uid = 0;
+    gs_render_cfg cfg{};
+    std::vector<int32_t> sizes;      // width, height per view
+    std::vector<uint8_t*> outs;
+    uint64_t layout = 0;             // context buffers the graph has baked in
+    cudaGraphExec_t exec = nullptr;
+    uint64_t last_use = 0;
+    int seen = 0;                    // calls with this key
+    int failed = 0;                  // capture failed: run this key without a graph
+};
+constexpr size_t kMaxGraphs = 8;
+
+std::atomic<uint64_t> g_scene_uid{1};
 
 }  // namespace
 
 struct gs_scene {
+    uint64_t uid = 0;  // never reused, unlike the address: keys the frame graphs
     int device = 0;
     int64_t n = 0;
     int32_t sh_degree = 0;
@@ -113,14 +138,19 @@ struct gs_ctx {
     DevBuf keys0, vals0, keys1, vals1;     // tile lists
     DevBuf sort_hist, sort_status;
     DevBuf ranges;
+    DevBuf tile_count, cursor;             // tile-bucket ordering: keys per tile, bucket fill cursors
     DevBuf counters;
     DevBuf image;                          // images of the host-output variants
     Counters* h_counters = nullptr;        // pinned mirror
+    Counters* h_init = nullptr;            // pinned per-frame reset image of the counters
     ViewParams* h_views = nullptr;         // pinned staging
     int h_views_cap = 0;
     cudaEvent_t ev[8] = {};
     int64_t key_capacity = 0;
     int64_t per_view_capacity = 0;         // Gaussians * views the splat buffers hold
+    cudaStream_t cap_stream = nullptr;     // graph capture
+    std::vector<FrameGraph> graphs;
+    uint64_t use_clock = 0;
 };
 
 namespace {
@@ -160,6 +190,7 @@ bool valid_cfg(const gs_render_cfg& c)
                        (c.tile_w == 8 && c.tile_h == 8);
     return shape && c.sh_max_degree >= 0 && c.sh_max_degree <= 3 && c.sort_variant >= 0 &&
            c.sort_variant < kSortVariants && c.views_per_block >= 0 &&
+           (c.ordering == GS_ORDER_BUCKETS || c.ordering == GS_ORDER_ONESWEEP) && (c.graph == 0 || c.graph == 1) &&
            (c.termination == GS_TERM_REFERENCE || c.termination == GS_TERM_TMIN);
 }
 
@@ -173,8 +204,19 @@ int eval_degree(const gs_scene* s, const gs_render_cfg& cfg) { return std::min(s
 float ms_between(cudaEvent_t a, cudaEvent_t b)
 {
     float ms = 0.f;
-    cudaEventElapsedTime(&ms, a, b);
+    if (cudaEventElapsedTime(&ms, a, b) != cudaSuccess) {
+        cudaGetLastError();  // not a frame failure: leave no error behind
+        ms = 0.f;
+    }
     return ms;
+}
+
+// Records `ev` on `st`; under stream capture as an event-record node of the
+// graph (an ordinary record would only become an internal dependency), so
+// replays can still be timed.
+cudaError_t record(cudaEvent_t ev, cudaStream_t st, bool capturing)
+{
+    return capturing ? cudaEventRecordWithFlags(ev, st, cudaEventRecordExternal) : cudaEventRecord(ev, st);
 }
 
 int ensure_sort_scratch(gs_ctx* ctx, int64_t num_items)
@@ -214,8 +256,24 @@ int ensure_ctx_host(gs_ctx* ctx, int num_views)
     return GS_OK;
 }
 
-// One frame over `num_views` views of `scene`.  outs[v] receives view v.
-int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
+// Grows the tile lists (both ping-pong pairs: tiles above the shared-memory
+// sort capacity use the second) to hold `keys` keys.
+int ensure_key_buffers(gs_ctx* ctx, int64_t keys)
+{
+    if (keys <= ctx->key_capacity && ctx->keys0.p) return GS_OK;
+    const size_t k = (size_t)std::max<int64_t>(keys, 1);
+    if (ctx->keys0.ensure(8 * k) || ctx->keys1.ensure(8 * k) || ctx->vals0.ensure(4 * k) || ctx->vals1.ensure(4 * k))
+        return fail(GS_ERR_OOM, "tile lists");
+    const int64_t cap = std::min(std::min((int64_t)(ctx->keys0.bytes / 8), (int64_t)(ctx->keys1.bytes / 8)),
+                                 std::min((int64_t)(ctx->vals0.bytes / 4), (int64_t)(ctx->vals1.bytes / 4)));
+    ctx->key_capacity = std::min<int64_t>(cap, (1ll << 31) - 1);
+    return GS_OK;
+}
+
+// One frame over `num_views` views of `scene` with GS_ORDER_ONESWEEP: keys
+// in Gaussian order at scanned offsets, radix sort, ranges.  The host reads
+// the exact key count between the projection and the emission.
+int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
               uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
 {
     if (!valid_cfg(cfg)) return fail(GS_ERR_INVALID, "invalid render cfg");
@@ -315,10 +373,8 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
 
     // 2. emit keys
     if (K > ctx->key_capacity) {
-        if (ctx->keys0.ensure(8 * (size_t)K) || ctx->keys1.ensure(8 * (size_t)K) || ctx->vals0.ensure(4 * (size_t)K) ||
-            ctx->vals1.ensure(4 * (size_t)K))
-            return fail(GS_ERR_OOM, "tile lists");
-        ctx->key_capacity = (int64_t)(ctx->keys0.bytes / 8);
+        rc = ensure_key_buffers(ctx, K);
+        if (rc) return rc;
     }
     rc = ensure_sort_scratch(ctx, K);
     if (rc) return rc;
@@ -402,6 +458,333 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     return GS_OK;
 }
 
+// ---- GS_ORDER_BUCKETS frames -------------------------------------------------
+
+// What the host decides before a tile-bucket frame is enqueued.
+struct FramePlan {
+    int num_views = 0;
+    int64_t n = 0, groups = 0, blocks = 0, items = 0, tiles_total = 0;
+    int vpb = 0, deg = 0;
+};
+
+// Validates the frame, fills the pinned view parameters and makes the
+// per-(view, Gaussian) and per-tile buffers large enough.
+int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views,
+                      const gs_render_cfg& cfg, uint8_t* const* outs, FramePlan& p)
+{
+    if (!valid_cfg(cfg)) return fail(GS_ERR_INVALID, "invalid render cfg");
+    if (num_views <= 0) return fail(GS_ERR_INVALID, "no views");
+    for (int v = 0; v < num_views; ++v) {
+        if (!valid_cam(&cams[v])) return fail(GS_ERR_INVALID, "invalid camera");
+        if (!outs[v]) return fail(GS_ERR_INVALID, "null output");
+    }
+    if (scene->sh_degree == 0 && !scene->color.p) return fail(GS_ERR_INVALID, "scene has no colour");
+    GS_CUDA(cudaSetDevice(ctx->device));
+    int rc = ensure_ctx_host(ctx, num_views);
+    if (rc) return rc;
+    p.num_views = num_views;
+    p.n = scene->n;
+    p.tiles_total = 0;
+    for (int v = 0; v < num_views; ++v) {
+        ViewParams& vp = ctx->h_views[v];
+        make_view_params(cams[v], cfg, vp);
+        vp.tile_offset = p.tiles_total;
+        vp.out = reinterpret_cast<uchar4*>(outs[v]);
+        p.tiles_total += (int64_t)vp.tiles_x * vp.tiles_y;
+    }
+    if (p.tiles_total >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many tiles");
+    p.items = p.n * num_views;
+    if (p.items >= (1ll << 31)) return fail(GS_ERR_INVALID, "views x Gaussians exceeds 2^31");
+    p.groups = (p.n + 255) / 256;
+    p.vpb = std::min(num_views, cfg.views_per_block > 0 ? cfg.views_per_block : 16);
+    p.blocks = p.groups * ((num_views + p.vpb - 1) / p.vpb);
+    p.deg = scene->sh_degree > 0 ? eval_degree(scene, cfg) : -1;
+
+    if (p.items > ctx->per_view_capacity) {
+        const size_t m = (size_t)p.items;
+        if (ctx->color.ensure(16 * m) || ctx->xy.ensure(8 * m) || ctx->z.ensure(4 * m) || ctx->ell.ensure(16 * m) ||
+            ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(4 * m) ||
+            ctx->rec.ensure(48 * m) || ctx->hitmask.ensure(4 * m))
+            return fail(GS_ERR_OOM, "splat buffers");
+        ctx->per_view_capacity = p.items;
+    }
+    const size_t tiles = (size_t)std::max<int64_t>(p.tiles_total, 1);
+    const size_t scan_blocks = (tiles + kTileScanItems - 1) / kTileScanItems;
+    if (sizeof(uint64_t) * scan_blocks > ctx->scan_status.bytes) {
+        if (ctx->scan_status.ensure(sizeof(uint64_t) * scan_blocks, true)) return fail(GS_ERR_OOM, "scan status");
+    }
+    if (ctx->ranges.ensure(sizeof(int32_t) * 2 * tiles) || ctx->tile_count.ensure(sizeof(uint32_t) * tiles) ||
+        ctx->cursor.ensure(sizeof(unsigned long long) * tiles))
+        return fail(GS_ERR_OOM, "tile buffers");
+    return GS_OK;
+}
+
+// Enqueues a whole tile-bucket frame on `st` with no host synchronisation
+// (everything a replayed graph needs): counters reset, fused projection,
+// tile scan, bucket emit, tile sort, raster, counters read-back into
+// ctx->h_counters.  The key count stays on the device; a frame whose keys
+// exceed ctx->key_capacity comes back with `overflow` set.
+int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg& cfg, const FramePlan& p,
+                         cudaStream_t st, bool capturing)
+{
+    Counters* dc = ctx->counters.as<Counters>();
+    GS_CUDA(cudaMemcpyAsync(ctx->views.p, ctx->h_views, sizeof(ViewParams) * p.num_views, cudaMemcpyHostToDevice, st));
+    GS_CUDA(cudaMemcpyAsync(dc, ctx->h_init, sizeof(Counters), cudaMemcpyHostToDevice, st));
+    GS_CUDA(cudaMemsetAsync(ctx->tile_count.p, 0, sizeof(uint32_t) * (size_t)p.tiles_total, st));
+    GS_CUDA(record(ctx->ev[0], st, capturing));
+
+    FrameArgs fa{};
+    fa.n = p.n;
+    fa.groups = p.groups;
+    fa.num_views = p.num_views;
+    fa.views_per_block = p.vpb;
+    fa.num_tiles = p.blocks;
+    fa.pos = scene->pos.as<float4>();
+    fa.sr = scene->sr.as<float4>();
+    fa.sh = scene->sh.as<float>();
+    fa.sh_count = scene->sh_count;
+    fa.color_in = scene->color.as<float4>();
+    fa.views = ctx->views.as<ViewParams>();
+    fa.raster_mode = cfg.termination;
+    fa.color = ctx->color.as<float4>();
+    fa.xy = ctx->xy.as<float2>();
+    fa.z = ctx->z.as<float>();
+    fa.ell = ctx->ell.as<float4>();
+    fa.conic = ctx->conic.as<float4>();
+    fa.rect = ctx->rect.as<int2>();
+    fa.rec = ctx->rec.as<float4>();
+    fa.hitmask = ctx->hitmask.as<uint32_t>();
+    fa.offsets = ctx->offsets.as<int32_t>();  // slot -> view * n + i
+    fa.err = &dc->err;
+    fa.tile_count = ctx->tile_count.as<uint32_t>();
+    fa.slot_counter = &dc->slots;
+    if (p.n > 0) launch_frame_project(fa, p.deg, st, true);
+
+    TileScanArgs ta{};
+    ta.count = ctx->tile_count.as<uint32_t>();
+    ta.tiles = p.tiles_total;
+    ta.cursor = ctx->cursor.as<unsigned long long>();
+    ta.ranges = ctx->ranges.as<int32_t>();
+    ta.status = ctx->scan_status.as<uint64_t>();
+    ta.block_counter = &dc->scan_block;
+    ta.epoch_dev = &dc->epoch_scan;
+    ta.err = &dc->err;
+    ta.total = &dc->total;
+    ta.capacity = ctx->key_capacity;
+    ta.sort_n = &dc->sort_n;
+    ta.overflow = &dc->overflow;
+    launch_tile_scan(ta, st);
+    GS_CUDA(record(ctx->ev[1], st, capturing));
+    GS_CUDA(record(ctx->ev[2], st, capturing));
+
+    BucketEmitArgs ea{};
+    ea.n = p.n;
+    ea.slot_count = &dc->slots;
+    ea.max_slots = p.items;
+    ea.views = ctx->views.as<ViewParams>();
+    ea.slot_gi = ctx->offsets.as<int32_t>();
+    ea.rect = ctx->rect.as<int2>();
+    ea.hitmask = ctx->hitmask.as<uint32_t>();
+    ea.xy = ctx->xy.as<float2>();
+    ea.ell = ctx->ell.as<float4>();
+    ea.z = ctx->z.as<float>();
+    ea.cursor = ctx->cursor.as<unsigned long long>();
+    ea.keys = ctx->keys0.as<uint64_t>();
+    ea.capacity = ctx->key_capacity;
+    if (p.n > 0) launch_emit_bucket(ea, ctx->num_sms, st);
+    GS_CUDA(record(ctx->ev[3], st, capturing));
+
+    TileSortArgs sa{};
+    sa.ranges = ctx->ranges.as<int32_t>();
+    sa.tiles = p.tiles_total;
+    sa.keys = ctx->keys0.as<uint64_t>();
+    sa.keys_alt = ctx->keys1.as<uint64_t>();
+    sa.vals = ctx->vals0.as<int32_t>();
+    sa.vals_alt = ctx->vals1.as<int32_t>();
+    sa.slot_gi = ctx->offsets.as<int32_t>();
+    if (p.n > 0) launch_tile_sort(sa, st);
+    GS_CUDA(record(ctx->ev[4], st, capturing));
+
+    RasterArgs ra{};
+    ra.view0 = ctx->h_views[0];
+    ra.views = ctx->views.as<ViewParams>();
+    ra.num_views = p.num_views;
+    ra.write_empty = 1;
+    ra.num_tiles_total = p.tiles_total;
+    ra.ranges = ctx->ranges.as<int32_t>();
+    ra.values = ctx->vals0.as<int32_t>();
+    ra.xy = ctx->xy.as<float2>();
+    ra.conic = ctx->conic.as<float4>();
+    ra.color = ctx->color.as<float4>();
+    ra.rec = cfg.termination == GS_TERM_TMIN ? ctx->rec.as<float4>() : nullptr;
+    ra.t_min = cfg.t_min;
+    ra.tile_counter = &dc->raster_tile;
+    launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, p.num_views > 1, ctx->num_sms, st);
+    GS_CUDA(cudaGetLastError());
+    GS_CUDA(record(ctx->ev[5], st, capturing));
+    GS_CUDA(cudaMemcpyAsync(ctx->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, st));
+    return GS_OK;
+}
+
+// Signature of every context buffer a captured frame refers to.
+uint64_t layout_of(const gs_ctx* ctx)
+{
+    const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
+                            &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->keys0, &ctx->vals0,
+                            &ctx->keys1, &ctx->vals1, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->counters};
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](uint64_t x) { h = (h ^ x) * 1099511628211ull; };
+    for (const DevBuf* b : bufs) {
+        mix((uint64_t)(uintptr_t)b->p);
+        mix((uint64_t)b->bytes);
+    }
+    mix((uint64_t)(uintptr_t)ctx->h_views);
+    mix((uint64_t)ctx->key_capacity);
+    return h;
+}
+
+bool same_frame(const FrameGraph& g, const gs_scene* scene, const gs_render_cfg& cfg, const gs_camera* cams,
+                int num_views, uint8_t* const* outs)
+{
+    if (g.scene_uid != scene->uid || (int)g.outs.size() != num_views) return false;
+    if (std::memcmp(&g.cfg, &cfg, sizeof(cfg)) != 0) return false;
+    for (int v = 0; v < num_views; ++v)
+        if (g.outs[v] != outs[v] || g.sizes[2 * v] != cams[v].width || g.sizes[2 * v + 1] != cams[v].height)
+            return false;
+    return true;
+}
+
+void drop_graph(FrameGraph& g)
+{
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g.exec = nullptr;
+}
+
+// Captures the frame enqueued by enqueue_bucket_frame into g.exec.
+bool capture_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg& cfg, const FramePlan& p, FrameGraph& g)
+{
+    if (!ctx->cap_stream && cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    if (cudaStreamBeginCapture(ctx->cap_stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    const int rc = enqueue_bucket_frame(ctx, scene, cfg, p, ctx->cap_stream, true);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(ctx->cap_stream, &graph);
+    bool ok = rc == GS_OK && e == cudaSuccess && graph;
+    if (ok) ok = cudaGraphInstantiate(&g.exec, graph, 0) == cudaSuccess;
+    if (graph) cudaGraphDestroy(graph);
+    if (!ok) {
+        g.exec = nullptr;
+        cudaGetLastError();
+    }
+    g.layout = layout_of(ctx);
+    return ok;
+}
+
+// One frame with GS_ORDER_BUCKETS.  The key count never goes to the host
+// before the frame ends: the lists are used at the capacity they have, and
+// a frame that outgrew them is redone once at 1.25x the count it reported.
+// With cfg.graph, the second frame with the same scene, options, view sizes
+// and outputs is captured into a CUDA graph and later ones replay it.
+int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
+                     uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
+{
+    FramePlan p;
+    int rc = plan_bucket_frame(ctx, scene, cams, num_views, cfg, outs, p);
+    if (rc) return rc;
+    if (!ctx->keys0.p) {
+        rc = ensure_key_buffers(ctx, std::max<int64_t>(p.items, 1 << 20));
+        if (rc) return rc;
+    }
+
+    // the graph slot of this frame, if any
+    FrameGraph* g = nullptr;
+    if (cfg.graph) {
+        for (FrameGraph& x : ctx->graphs)
+            if (same_frame(x, scene, cfg, cams, num_views, outs)) g = &x;
+        if (!g) {
+            if (ctx->graphs.size() >= kMaxGraphs) {
+                auto lru = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
+                                            [](const FrameGraph& a, const FrameGraph& b) { return a.last_use < b.last_use; });
+                drop_graph(*lru);
+                ctx->graphs.erase(lru);
+            }
+            ctx->graphs.emplace_back();
+            g = &ctx->graphs.back();
+            g->scene_uid = scene->uid;
+            g->cfg = cfg;
+            g->outs.assign(outs, outs + num_views);
+            g->sizes.resize(2 * (size_t)num_views);
+            for (int v = 0; v < num_views; ++v) {
+                g->sizes[2 * v] = cams[v].width;
+                g->sizes[2 * v + 1] = cams[v].height;
+            }
+        } else if (g->exec && g->layout != layout_of(ctx)) {
+            drop_graph(*g);  // buffers moved since the capture
+        }
+        g->last_use = ++ctx->use_clock;
+        ++g->seen;
+    }
+
+    int attempts = 0;
+    bool replayed = false;
+    for (;;) {
+        ++attempts;
+        ctx->h_init->epoch_scan = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
+        ctx->h_init->epoch_sort = 0;
+        // the second call with the same key is captured; a redone frame is not
+        const bool use_graph = g && !g->failed && g->seen >= 2 && attempts == 1;
+        if (use_graph && !g->exec && !capture_frame(ctx, scene, cfg, p, *g)) g->failed = 1;
+        if (use_graph && g->exec) {
+            GS_CUDA(cudaGraphLaunch(g->exec, st));
+            replayed = true;
+        } else {
+            rc = enqueue_bucket_frame(ctx, scene, cfg, p, st, false);
+            if (rc) return rc;
+            replayed = false;
+        }
+        GS_CUDA(cudaStreamSynchronize(st));
+        if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "frame look-back timed out");
+        const int64_t K = ctx->h_counters->total;
+        if (K >= (1ll << 31)) return fail(GS_ERR_CAPACITY, "more than 2^31 tile keys");
+        if (!ctx->h_counters->overflow) break;
+        if (attempts >= 2) return fail(GS_ERR_CUDA, "tile list overflow after regrowing");
+        if (g) drop_graph(*g);
+        rc = ensure_key_buffers(ctx, std::min<int64_t>(K + K / 4, (1ll << 31) - 1));
+        if (rc) return rc;
+    }
+
+    if (stats) {
+        stats->sh_eval_ms = 0.0;
+        stats->project_ms = ms_between(ctx->ev[0], ctx->ev[1]);
+        stats->build_tile_ms = ms_between(ctx->ev[2], ctx->ev[3]);
+        stats->sort_ms = ms_between(ctx->ev[3], ctx->ev[4]);
+        stats->raster_ms = ms_between(ctx->ev[4], ctx->ev[5]);
+        stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
+        stats->num_keys = ctx->h_counters->total;
+        stats->num_tiles = p.tiles_total;
+        // frame kernel, tile scan, bucket emit, tile sort, raster
+        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 2;
+        stats->graph_replay = replayed ? 1 : 0;
+        stats->attempts = attempts;
+    }
+    return GS_OK;
+}
+
+int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
+              uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
+{
+    if (cfg.ordering == GS_ORDER_ONESWEEP) {
+        if (stats) stats->graph_replay = 0, stats->attempts = 1;
+        return run_frame_onesweep(ctx, scene, cams, num_views, cfg, outs, stats, st);
+    }
+    return run_frame_bucket(ctx, scene, cams, num_views, cfg, outs, stats, st);
+}
+
 }  // namespace
 
 // ============================================================================
@@ -436,8 +819,10 @@ void gs_default_cfg(gs_render_cfg* cfg)
     cfg->t_min = 1e-4f;
     cfg->tile_w = 16;
     cfg->tile_h = 16;
+    cfg->ordering = GS_ORDER_BUCKETS;
     cfg->sort_variant = 0;
     cfg->views_per_block = 0;
+    cfg->graph = 1;
 }
 
 void gs_camera_look_at(gs_camera* cam, const float eye[3], const float target[3], const float up[3], float fovy_rad,
@@ -496,11 +881,15 @@ int gs_ctx_create(int device, gs_ctx** out)
         delete c;
         return fail(GS_ERR_OOM, "counters");
     }
-    if (cudaMallocHost(&c->h_counters, sizeof(Counters)) != cudaSuccess) {
+    if (cudaMallocHost(&c->h_counters, sizeof(Counters)) != cudaSuccess ||
+        cudaMallocHost(&c->h_init, sizeof(Counters)) != cudaSuccess) {
+        if (c->h_counters) cudaFreeHost(c->h_counters);
         c->counters.release();
         delete c;
         return fail(GS_ERR_OOM, "pinned counters");
     }
+    std::memset(c->h_init, 0, sizeof(Counters));
+    std::memset(c->h_counters, 0, sizeof(Counters));
     for (auto& ev : c->ev) cudaEventCreate(&ev);
     *out = c;
     return GS_OK;
@@ -511,11 +900,15 @@ int gs_ctx_destroy(gs_ctx* ctx)
     if (!ctx) return GS_OK;
     cudaSetDevice(ctx->device);
     cudaDeviceSynchronize();
+    for (FrameGraph& g : ctx->graphs) drop_graph(g);
+    ctx->graphs.clear();
+    if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                       &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
-                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
+                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->counters, &ctx->image};
     for (DevBuf* b : bufs) b->release();
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
+    if (ctx->h_init) cudaFreeHost(ctx->h_init);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     for (auto& ev : ctx->ev)
         if (ev) cudaEventDestroy(ev);
@@ -528,7 +921,7 @@ int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
     if (!ctx) return 0;
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                             &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
-                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->counters, &ctx->image};
+                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->counters, &ctx->image};
     int64_t t = 0;
     for (const DevBuf* b : bufs) t += (int64_t)b->bytes;
     return t;
@@ -546,6 +939,7 @@ int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float
     GS_CUDA(cudaSetDevice(ctx->device));
     gs_scene* s = new (std::nothrow) gs_scene();
     if (!s) return fail(GS_ERR_OOM, "host allocation");
+    s->uid = g_scene_uid.fetch_add(1);
     s->device = ctx->device;
     s->n = n;
     s->sh_degree = sh_degree;
@@ -808,6 +1202,9 @@ int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_
 {
     if (!valid_cam(cam) || !cfg || !d_ranges || !d_rgba) return fail(GS_ERR_INVALID, "bad argument");
     if (!valid_cfg(*cfg)) return fail(GS_ERR_INVALID, "invalid render cfg");
+    // entries are staged with 8- and 16-byte asynchronous copies
+    if (((uintptr_t)d_xy & 7) || ((uintptr_t)d_conic & 15) || ((uintptr_t)d_color & 15))
+        return fail(GS_ERR_INVALID, "xy must be 8-byte and conic/color 16-byte aligned");
     RasterArgs ra = {};
     make_view_params(*cam, *cfg, ra.view0);
     ra.view0.out = reinterpret_cast<uchar4*>(d_rgba);

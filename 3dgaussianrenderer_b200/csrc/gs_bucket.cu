@@ -1,0 +1,547 @@
+// Tile-bucket ordering of the frame pipeline: the whole-frame replacement
+// for the reference's buildTileList + sortTileList + evaluateTileRanges
+// (core/gaussian_render.cu:312-677).
+//
+// The reference emits (tile << 32 | depth, index) keys, radix-sorts all of
+// them on tile and depth bits, then finds each tile's range.  Here the frame
+// kernel has already counted every tile's keys, so:
+//   1. tile scan   -- exclusive scan of the tile counts = each tile's range;
+//   2. bucket emit -- every overlap is written straight into its tile's
+//                     range, at a position claimed with one atomic, as
+//                     (depth << 32 | slot);
+//   3. tile sort   -- one CTA per tile orders the tile's keys by depth in
+//                     shared memory (LSD radix over only the depth bits that
+//                     vary inside the tile), then, if two keys of the tile
+//                     share a depth, re-sorts on (depth, view * n + i).
+// The result per tile is exactly the order of a stable sort of the
+// reference's keys emitted in Gaussian order: depth first, index among equal
+// depths.  Each key crosses HBM about three times (emit, sort read, sorted
+// index write) instead of twice per radix pass.
+#include "gs_kernels.h"
+
+#include <algorithm>
+
+namespace gs {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+
+// Exclusive block scan of one int64 per thread; every thread must call it.
+__device__ __forceinline__ int64_t excl_scan_block(const int64_t v, int64_t* s_tmp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int64_t incl = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int64_t t = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) s_tmp[warp] = incl;
+    __syncthreads();
+    int64_t prefix = 0;
+    for (int w = 0; w < warp; ++w) prefix += s_tmp[w];
+    __syncthreads();
+    return prefix + incl - v;
+}
+
+// OR and AND of one 64-bit value per thread over the block (pads pass
+// or_v = 0, and_v = ~0); every thread must call it.
+__device__ __forceinline__ uint64_t varying_bits_block(uint64_t or_v, uint64_t and_v, uint64_t* s_tmp)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 16; o >= 1; o >>= 1) {
+        or_v |= __shfl_xor_sync(kFull, or_v, o);
+        and_v &= __shfl_xor_sync(kFull, and_v, o);
+    }
+    if (lane == 0) {
+        s_tmp[warp] = or_v;
+        s_tmp[kWarps + warp] = and_v;
+    }
+    __syncthreads();
+    uint64_t o = 0, n = ~0ull;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        o |= s_tmp[w];
+        n &= s_tmp[kWarps + w];
+    }
+    __syncthreads();
+    return o ^ n;
+}
+
+}  // namespace
+
+// ---- 1. tile scan -------------------------------------------------------------
+
+__global__ void __launch_bounds__(kThreads) tile_scan_kernel(TileScanArgs a)
+{
+    constexpr int IPT = kTileScanItems / kThreads;
+    __shared__ int64_t s_tmp[kWarps];
+    __shared__ int64_t s_base;
+    __shared__ int64_t s_blk;
+    if (threadIdx.x == 0) s_blk = (int64_t)atomicAdd(a.block_counter, 1ull);
+    __syncthreads();
+    const int64_t blk = s_blk;
+    const int64_t nblk = (a.tiles + kTileScanItems - 1) / kTileScanItems;
+    if (blk >= nblk) return;
+    const uint32_t epoch = a.epoch_dev ? *a.epoch_dev : a.epoch;
+
+    // thread t owns tiles [first, first + IPT) of this block
+    const int64_t first = blk * kTileScanItems + (int64_t)threadIdx.x * IPT;
+    uint32_t c[IPT];
+    int64_t sum = 0;
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+        c[j] = first + j < a.tiles ? __ldg(&a.count[first + j]) : 0u;
+        sum += c[j];
+    }
+    const int64_t excl = excl_scan_block(sum, s_tmp);
+    if (threadIdx.x == kThreads - 1) {
+        const uint64_t agg = (uint64_t)(excl + sum);
+        uint64_t prev = 0;
+        uint64_t* st = a.status + blk;
+        if (blk == 0) {
+            store_status(st, status_word(kFlagP, epoch, agg));
+        } else {
+            store_status(st, status_word(kFlagA, epoch, agg));
+            prev = look_back(a.status, blk, 1, epoch, a.err, kErrTimeout);
+            store_status(st, status_word(kFlagP, epoch, prev + agg));
+        }
+        s_base = (int64_t)prev;
+        if (blk == nblk - 1) {
+            const int64_t total = (int64_t)(prev + agg);
+            *a.total = total;
+            if (a.sort_n) {
+                *a.sort_n = total < a.capacity ? total : a.capacity;
+                *a.overflow = total > a.capacity ? 1 : 0;
+            }
+        }
+    }
+    __syncthreads();
+    int64_t run = s_base + excl;
+    const int64_t cap = a.capacity;
+#pragma unroll
+    for (int j = 0; j < IPT; ++j) {
+        const int64_t t = first + j;
+        if (t < a.tiles) {
+            a.cursor[t] = (unsigned long long)run;
+            const int64_t lo = run < cap ? run : cap;
+            const int64_t hi = run + c[j] < cap ? run + c[j] : cap;
+            a.ranges[2 * t] = (int32_t)lo;
+            a.ranges[2 * t + 1] = (int32_t)hi;
+        }
+        run += c[j];
+    }
+}
+
+void launch_tile_scan(const TileScanArgs& a, cudaStream_t st)
+{
+    const int64_t blocks = (a.tiles + kTileScanItems - 1) / kTileScanItems;
+    if (blocks <= 0) return;
+    tile_scan_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(a);
+}
+
+// ---- 2. bucket emit -----------------------------------------------------------
+
+__device__ __forceinline__ uint32_t depth_bits(const float depth)
+{
+    return (uint32_t)(make_key(0, depth) & 0xFFFFFFFFull);
+}
+
+__device__ __forceinline__ void put_key(const BucketEmitArgs& a, const int64_t gtile, const uint32_t depth,
+                                        const int64_t slot)
+{
+    const unsigned long long pos = atomicAdd(&a.cursor[gtile], 1ull);
+    if ((int64_t)pos < a.capacity) a.keys[pos] = ((uint64_t)depth << 32) | (uint32_t)slot;
+}
+
+// Grid-strided over the slots in 256-slot steps (the slot count is only
+// known on the device).  Rectangles of at most 32 candidates expand the hit
+// mask the frame kernel recorded; larger ones are re-tested by the whole
+// warp, 32 candidates at a time.
+__global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
+{
+    const int64_t nslots = (int64_t)*a.slot_count;
+    const int lane = threadIdx.x & 31;
+    for (int64_t base = (int64_t)blockIdx.x * kThreads; base < nslots; base += (int64_t)gridDim.x * kThreads) {
+        const int64_t slot = base + threadIdx.x;
+        int cand = 0, view = 0;
+        int4 r = make_int4(0, 0, 0, 0);
+        Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        uint32_t depth = 0;
+        if (slot < nslots) {
+            view = (int)((int64_t)__ldg(&a.slot_gi[slot]) / a.n);
+            r = unpack_rect(__ldg(&a.rect[slot]));
+            cand = rect_candidates(r);
+            depth = depth_bits(__ldg(&a.z[slot]));
+            if (cand <= 32) {
+                const ViewParams& v = a.views[view];
+                uint32_t m = __ldg(&a.hitmask[slot]);
+                while (m) {
+                    const int c = __ffs(m) - 1;
+                    m &= m - 1;
+                    const int gx = r.x + c % r.z, gy = r.y + c / r.z;
+                    put_key(a, v.tile_offset + gy * v.tiles_x + gx, depth, slot);
+                }
+                cand = 0;
+            } else {
+                const float2 c = __ldg(&a.xy[slot]);
+                const float4 el = __ldg(&a.ell[slot]);
+                e = {c.x, c.y, el.x, el.y, el.z, el.w};
+            }
+        }
+        if (__ballot_sync(kFull, cand > 0) == 0) continue;
+        // warp-cooperative walk over the large rectangles
+        int incl = cand;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, o);
+            if (lane >= o) incl += t;
+        }
+        const int excl = incl - cand;
+        const int total = __shfl_sync(kFull, incl, 31);
+        for (int cb = 0; cb < total; cb += 32) {
+            const int c = cb + lane;
+            int o = 0;
+#pragma unroll
+            for (int b = 16; b >= 1; b >>= 1) {
+                const int t = __shfl_sync(kFull, incl, o + b - 1);
+                if (t <= c) o += b;
+            }
+            Ell oe;
+            oe.cx = __shfl_sync(kFull, e.cx, o);
+            oe.cy = __shfl_sync(kFull, e.cy, o);
+            oe.cs = __shfl_sync(kFull, e.cs, o);
+            oe.sn = __shfl_sync(kFull, e.sn, o);
+            oe.ex = __shfl_sync(kFull, e.ex, o);
+            oe.ey = __shfl_sync(kFull, e.ey, o);
+            int4 orr;
+            orr.x = __shfl_sync(kFull, r.x, o);
+            orr.y = __shfl_sync(kFull, r.y, o);
+            orr.z = __shfl_sync(kFull, r.z, o);
+            orr.w = __shfl_sync(kFull, r.w, o);
+            const int oexcl = __shfl_sync(kFull, excl, o);
+            const int oview = __shfl_sync(kFull, view, o);
+            const uint32_t od = __shfl_sync(kFull, depth, o);
+            if (c < total) {
+                int tile = 0;
+                const ViewParams& v = a.views[oview];
+                if (candidate_hit(oe, orr, c - oexcl, v, tile))
+                    put_key(a, v.tile_offset + tile, od, base + (threadIdx.x & ~31) + o);
+            }
+        }
+    }
+}
+
+void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st)
+{
+    const int64_t blocks = std::min<int64_t>((a.max_slots + kThreads - 1) / kThreads, (int64_t)num_sms * 16);
+    if (blocks <= 0) return;
+    emit_bucket_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(a);
+}
+
+// ---- 3. tile sort ---------------------------------------------------------------
+
+namespace {
+
+struct SortSmem {
+    uint64_t* k;       // [kTileSortSmemKeys]; the warp histograms alias it while ranking
+    int32_t* v;        // [kTileSortSmemKeys]
+    uint32_t* whist;   // [kWarps][256] (aliases k)
+    int32_t* bexcl;    // [256] digit start inside the ranked chunk
+    int32_t* dcount;   // [256] digit count of the ranked chunk
+    int64_t* scan;     // [kWarps]
+    uint64_t* red;     // [2 * kWarps]
+    int32_t* run;      // [256] running digit start (global-memory passes)
+};
+
+// Stable rank of IPT keys per thread by the digit (key >> shift) & 0xFF.
+// Item order: p = warp * 32 * IPT + i * 32 + lane.  pos[i] = rank of item i
+// in the chunk; sm.bexcl / sm.dcount hold each digit's start and count.
+// Every thread must call it; it ends with a barrier.
+template <int IPT>
+__device__ __forceinline__ void block_rank(const uint64_t (&key)[IPT], const int shift, int (&pos)[IPT],
+                                           const SortSmem& sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* wh = sm.whist + warp * 256;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) wh[lane + 32 * k] = 0;
+    __syncwarp();
+    const unsigned lt = lanemask_lt();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const unsigned d = (unsigned)(key[i] >> shift) & 0xFFu;
+        unsigned peers = kFull;
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const unsigned bal = __ballot_sync(kFull, (d >> b) & 1u);
+            peers &= ((d >> b) & 1u) ? bal : ~bal;
+        }
+        const uint32_t before = wh[d];
+        const int below = __popc(peers & lt);
+        __syncwarp();
+        if (below == 0) wh[d] = before + __popc(peers);
+        __syncwarp();
+        pos[i] = (int)before + below;
+    }
+    __syncthreads();
+    const int d = threadIdx.x;  // 256 threads = 256 digits
+    int run = 0;
+#pragma unroll
+    for (int w = 0; w < kWarps; ++w) {
+        const uint32_t c = sm.whist[w * 256 + d];
+        sm.whist[w * 256 + d] = (uint32_t)run;
+        run += (int)c;
+    }
+    const int ex = (int)excl_scan_block((int64_t)run, sm.scan);
+    sm.bexcl[d] = ex;
+    sm.dcount[d] = run;
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const unsigned dd = (unsigned)(key[i] >> shift) & 0xFFu;
+        pos[i] += sm.bexcl[dd] + (int)sm.whist[warp * 256 + dd];
+    }
+    __syncthreads();  // whist (aliasing k) may be overwritten from here on
+}
+
+// LSD passes over the 8-bit windows that cover `mask`, lowest first; the
+// data lives in registers (p order) and goes through shared memory between
+// passes.  Returns with registers and sm.k / sm.v in sorted p order when at
+// least one pass ran.
+template <int IPT>
+__device__ __forceinline__ bool smem_sort(uint64_t (&k)[IPT], int32_t (&v)[IPT], uint64_t mask, const SortSmem& sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    bool any = false;
+    while (mask) {
+        const int shift = __ffsll((long long)mask) - 1;
+        mask &= ~(0xFFull << shift);
+        int pos[IPT];
+        block_rank<IPT>(k, shift, pos, sm);
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            sm.k[pos[i]] = k[i];
+            sm.v[pos[i]] = v[i];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int p = warp * 32 * IPT + i * 32 + lane;
+            k[i] = sm.k[p];
+            v[i] = sm.v[p];
+        }
+        __syncthreads();
+        any = true;
+    }
+    return any;
+}
+
+template <int IPT>
+__device__ void sort_tile_smem(const TileSortArgs& a, const int64_t start, const int m, const SortSmem& sm)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t k[IPT];
+    int32_t v[IPT];
+    uint64_t o = 0, n = ~0ull;
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const int p = warp * 32 * IPT + i * 32 + lane;
+        if (p < m) {
+            k[i] = a.keys[start + p];
+            v[i] = (int32_t)(uint32_t)k[i];
+            o |= k[i];
+            n &= k[i];
+        } else {
+            k[i] = ~0ull;  // pads rank last and are never written
+            v[i] = 0;
+        }
+    }
+    const uint64_t vary = varying_bits_block(o, n, sm.red) & 0xFFFFFFFF00000000ull;
+    bool tie;
+    if (smem_sort<IPT>(k, v, vary, sm)) {
+        bool t = false;
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int p = warp * 32 * IPT + i * 32 + lane;
+            if (p >= 1 && p < m) t |= (sm.k[p] >> 32) == (sm.k[p - 1] >> 32);
+        }
+        tie = __syncthreads_or(t) != 0;
+    } else {
+        tie = true;  // one depth for the whole tile (m >= 2)
+    }
+    if (tie) {
+        // order equal depths by view * n + i: sort again on (depth, index)
+        o = 0;
+        n = ~0ull;
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int p = warp * 32 * IPT + i * 32 + lane;
+            if (p < m) {
+                k[i] = (k[i] & 0xFFFFFFFF00000000ull) | (uint32_t)__ldg(&a.slot_gi[v[i]]);
+                o |= k[i];
+                n &= k[i];
+            }
+        }
+        smem_sort<IPT>(k, v, varying_bits_block(o, n, sm.red), sm);
+    }
+#pragma unroll
+    for (int i = 0; i < IPT; ++i) {
+        const int p = warp * 32 * IPT + i * 32 + lane;
+        if (p < m) a.vals[start + p] = v[i];
+    }
+}
+
+// One stable LSD pass of a tile too large for shared memory, by one CTA:
+// digit histogram of the segment, then 4096-key chunks in order, each
+// ranked in the block and written at its digits' running starts.
+__device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t* out_k, int32_t* out_v, const int m,
+                            const int shift, const SortSmem& sm)
+{
+    constexpr int IPT = kTileSortSmemKeys / kThreads;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(sm.v);  // the value buffer is unused on this path
+    hist[threadIdx.x] = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < m; p += kThreads) atomicAdd(&hist[(unsigned)(in_k[p] >> shift) & 0xFFu], 1u);
+    __syncthreads();
+    const int ex = (int)excl_scan_block((int64_t)hist[threadIdx.x], sm.scan);
+    sm.run[threadIdx.x] = ex;
+    __syncthreads();
+    for (int c0 = 0; c0 < m; c0 += kTileSortSmemKeys) {
+        uint64_t k[IPT];
+        int32_t v[IPT];
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int p = c0 + warp * 32 * IPT + i * 32 + lane;
+            if (p < m) {
+                k[i] = in_k[p];
+                v[i] = in_v ? in_v[p] : (int32_t)(uint32_t)k[i];
+            } else {
+                k[i] = ~0ull;
+                v[i] = 0;
+            }
+        }
+        int pos[IPT];
+        block_rank<IPT>(k, shift, pos, sm);
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int p = c0 + warp * 32 * IPT + i * 32 + lane;
+            if (p < m) {
+                const unsigned d = (unsigned)(k[i] >> shift) & 0xFFu;
+                const int dst = sm.run[d] + (pos[i] - sm.bexcl[d]);
+                out_k[dst] = k[i];
+                out_v[dst] = v[i];
+            }
+        }
+        __syncthreads();
+        sm.run[threadIdx.x] += sm.dcount[threadIdx.x];
+        __syncthreads();
+    }
+}
+
+__device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, const int m, const SortSmem& sm)
+{
+    uint64_t* bk[2] = {a.keys + start, a.keys_alt + start};
+    int32_t* bv[2] = {a.vals + start, a.vals_alt + start};
+    int cur = 0;
+    bool have_v = false;  // values not yet materialised: slot = low key bits
+
+    auto vary_of = [&](const uint64_t hi_mask) {
+        uint64_t o = 0, n = ~0ull;
+        for (int p = threadIdx.x; p < m; p += kThreads) {
+            const uint64_t x = bk[cur][p];
+            o |= x;
+            n &= x;
+        }
+        return varying_bits_block(o, n, sm.red) & hi_mask;
+    };
+    auto run_passes = [&](uint64_t mask) {
+        while (mask) {
+            const int shift = __ffsll((long long)mask) - 1;
+            mask &= ~(0xFFull << shift);
+            global_pass(bk[cur], have_v ? bv[cur] : nullptr, bk[cur ^ 1], bv[cur ^ 1], m, shift, sm);
+            cur ^= 1;
+            have_v = true;
+        }
+    };
+
+    run_passes(vary_of(0xFFFFFFFF00000000ull));
+    bool t = false;
+    for (int p = threadIdx.x + 1; p < m; p += kThreads) t |= (bk[cur][p] >> 32) == (bk[cur][p - 1] >> 32);
+    if (__syncthreads_or(t)) {
+        for (int p = threadIdx.x; p < m; p += kThreads) {
+            const uint64_t x = bk[cur][p];
+            const int32_t s = have_v ? bv[cur][p] : (int32_t)(uint32_t)x;
+            bv[cur][p] = s;
+            bk[cur][p] = (x & 0xFFFFFFFF00000000ull) | (uint32_t)__ldg(&a.slot_gi[s]);
+        }
+        have_v = true;
+        __syncthreads();
+        run_passes(vary_of(~0ull));
+    }
+    // result into a.vals
+    if (!have_v) {
+        for (int p = threadIdx.x; p < m; p += kThreads) bv[0][p] = (int32_t)(uint32_t)bk[cur][p];
+    } else if (cur == 1) {
+        for (int p = threadIdx.x; p < m; p += kThreads) bv[0][p] = bv[1][p];
+    }
+}
+
+}  // namespace
+
+// One CTA per tile; the tile's key count picks the shared-memory size class.
+__global__ void __launch_bounds__(kThreads, 2) tile_sort_kernel(TileSortArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int32_t s_bexcl[256];
+    __shared__ int32_t s_dcount[256];
+    __shared__ int32_t s_run[256];
+    __shared__ int64_t s_scan[kWarps];
+    __shared__ uint64_t s_red[2 * kWarps];
+    const int64_t t = blockIdx.x;
+    const int64_t start = __ldg(&a.ranges[2 * t]);
+    const int m = __ldg(&a.ranges[2 * t + 1]) - (int)start;
+    if (m <= 1) {
+        if (m == 1 && threadIdx.x == 0) a.vals[start] = (int32_t)(uint32_t)a.keys[start];
+        return;
+    }
+    SortSmem sm;
+    sm.k = reinterpret_cast<uint64_t*>(smem);
+    sm.v = reinterpret_cast<int32_t*>(smem + kTileSortSmemKeys * 8);
+    sm.whist = reinterpret_cast<uint32_t*>(smem);
+    sm.bexcl = s_bexcl;
+    sm.dcount = s_dcount;
+    sm.scan = s_scan;
+    sm.red = s_red;
+    sm.run = s_run;
+    if (m <= 256)
+        sort_tile_smem<1>(a, start, m, sm);
+    else if (m <= 512)
+        sort_tile_smem<2>(a, start, m, sm);
+    else if (m <= 1024)
+        sort_tile_smem<4>(a, start, m, sm);
+    else if (m <= 2048)
+        sort_tile_smem<8>(a, start, m, sm);
+    else if (m <= kTileSortSmemKeys)
+        sort_tile_smem<16>(a, start, m, sm);
+    else
+        sort_tile_global(a, start, m, sm);
+}
+
+void launch_tile_sort(const TileSortArgs& a, cudaStream_t st)
+{
+    constexpr int smem = kTileSortSmemKeys * 12;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(tile_sort_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        attr = true;
+    }
+    if (a.tiles <= 0) return;
+    tile_sort_kernel<<<(unsigned)a.tiles, kThreads, smem, st>>>(a);
+}
+
+}  // namespace gs

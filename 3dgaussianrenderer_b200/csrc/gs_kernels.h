@@ -42,7 +42,68 @@ struct FrameArgs {
     unsigned long long* tile_counter;
     int64_t* view_total;  // [num_views] keys per view
     int* err;
+    // tile-bucket pipeline (launch_frame_project with bucket = true): the
+    // (view, Gaussian) pairs that overlap a tile take slots from
+    // `slot_counter` in any order; every per-item output above is written
+    // at the slot instead of view * n + i, `offsets[slot]` receives
+    // view * n + i, and each overlapped tile's key count is added to
+    // tile_count[view tile offset + tile].
+    uint32_t* tile_count;
+    unsigned long long* slot_counter;
 };
+
+// Bucket emission: every overlap of slot s is written as
+// (depth bits << 32 | s) at an atomically claimed position of its tile's
+// bucket (cursor[tile], preset to the tile's first key by the tile scan).
+struct BucketEmitArgs {
+    int64_t n;                       // Gaussians per view
+    const unsigned long long* slot_count;
+    int64_t max_slots;               // grid bound
+    const ViewParams* views;
+    const int32_t* slot_gi;          // view * n + i of each slot
+    const int2* rect;
+    const uint32_t* hitmask;
+    const float2* xy;
+    const float4* ell;
+    const float* z;
+    unsigned long long* cursor;      // [tiles]
+    uint64_t* keys;
+    int64_t capacity;
+};
+
+// Exclusive scan of the per-tile key counts into tile ranges and bucket
+// cursors; the last block writes the key total.  Ranges are clamped to
+// `capacity` (a frame whose keys do not fit is flagged, never overrun).
+struct TileScanArgs {
+    const uint32_t* count;           // [tiles]
+    int64_t tiles;
+    unsigned long long* cursor;      // [tiles] out: first key of the tile
+    int32_t* ranges;                 // [2 * tiles] out: first, one past last
+    uint64_t* status;                // look-back words, one per 4096 tiles
+    unsigned long long* block_counter;
+    uint32_t epoch;
+    const uint32_t* epoch_dev;       // non-null: epoch read here
+    int* err;
+    int64_t* total;                  // K
+    int64_t capacity;
+    int64_t* sort_n;                 // min(K, capacity)
+    int* overflow;                   // K > capacity
+};
+
+// Per-tile sort of the buckets: each tile's keys are ordered by depth and,
+// among equal depths, by view * n + i, which is the order of a stable sort
+// of the reference's (tile | depth) keys emitted in Gaussian order.
+struct TileSortArgs {
+    const int32_t* ranges;
+    int64_t tiles;
+    uint64_t* keys;                  // bucketed (depth << 32 | slot); reordered in place
+    uint64_t* keys_alt;              // scratch for tiles above the shared-memory capacity
+    int32_t* vals;                   // out: slots in blend order
+    int32_t* vals_alt;
+    const int32_t* slot_gi;
+};
+constexpr int kTileSortSmemKeys = 4096;
+constexpr int kTileScanItems = 4096;  // tiles per scan block
 
 struct EmitArgs {
     int64_t n;
@@ -106,7 +167,10 @@ void launch_sh_stage(int64_t n, const float4* pos, const float* sh, int sh_count
                      float4* color, cudaStream_t st);
 void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const ViewParams& v, float2* xy,
                           float* z, float4* ell, float4* conic, cudaStream_t st);
-void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st);
+void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st, bool bucket = false);
+void launch_tile_scan(const TileScanArgs& a, cudaStream_t st);
+void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st);
+void launch_tile_sort(const TileSortArgs& a, cudaStream_t st);
 void launch_count_stage(const FrameArgs& a, cudaStream_t st);
 // view_base[v] = sum of view_total[u < v]; *total = sum of all.  With a
 // non-null `sort_n`, also *sort_n = min(total, capacity) and *overflow = 1

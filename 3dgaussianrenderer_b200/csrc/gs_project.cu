@@ -92,8 +92,10 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
 
 // Returns this lane's number of overlapping tiles; for rectangles of at
 // most 32 candidates also the hit mask (bit c = candidate c overlaps).
+// With a non-null `tile_count`, every overlap also adds one to its tile's
+// count (all lanes of the warp render the same view).
 __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
-                                               uint32_t& mask)
+                                               uint32_t& mask, uint32_t* tile_count = nullptr)
 {
     const int lane = threadIdx.x & 31;
     const WarpCands w = warp_scan_cands(cand);
@@ -119,6 +121,7 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
         if (c < w.total) {
             int tile;
             hit = candidate_hit(oe, orr, c - oexcl, v, tile);
+            if (hit && tile_count) atomicAdd(&tile_count[v.tile_offset + tile], 1u);
         }
         const unsigned bal = __ballot_sync(kFull, hit);
         const unsigned bits = bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32));
@@ -195,12 +198,16 @@ __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
 // SH colour, projection, tile rectangle, exact overlap count, and the
 // within-view key offset from that view's look-back chain.  Gaussians that
 // overlap no tile write only their offset.
-template <int DEG>
+//
+// BUCKET: no scan at all -- each overlapping (view, Gaussian) takes a slot
+// (one atomic per warp) and adds its overlaps to the per-tile counts; the
+// blocks are independent and run in launch order.
+template <int DEG, bool BUCKET>
 __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
 {
     extern __shared__ __align__(128) float s_sh[];  // [3*(DEG+1)^2][256]
     __shared__ __align__(8) uint64_t s_bar;
-    const int64_t tile = acquire_tile(a.tile_counter);
+    const int64_t tile = BUCKET ? (int64_t)blockIdx.x : acquire_tile(a.tile_counter);
     const int64_t chunk = tile / a.groups;
     const int64_t group = tile - chunk * a.groups;
     const int64_t i = group * 256 + threadIdx.x;
@@ -255,11 +262,23 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
             cand = rect_candidates(r);
         }
         uint32_t mask;
-        const int hits = warp_count_hits(e, r, cand, v, mask);
-        const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, epoch,
-                                          a.view_total + view, a.err);
+        const int hits = warp_count_hits(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr);
+        int64_t o_out = o;  // where this item's outputs go
+        if (BUCKET) {
+            const unsigned bal = __ballot_sync(kFull, hits > 0);
+            if (bal == 0) continue;  // warp-uniform
+            unsigned long long first = 0;
+            if ((threadIdx.x & 31) == 0) first = atomicAdd(a.slot_counter, (unsigned long long)__popc(bal));
+            first = __shfl_sync(kFull, first, 0);
+            o_out = (int64_t)first + __popc(bal & lanemask_lt());
+            if (hits > 0) a.offsets[o_out] = (int32_t)o;
+        } else {
+            const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, epoch,
+                                              a.view_total + view, a.err);
+            if (valid) a.offsets[o] = (int32_t)off;
+        }
         if (valid) {
-            a.offsets[o] = (int32_t)off;
+            const int64_t o = o_out;
             if (hits > 0) {
                 a.z[o] = s.z;
                 a.rect[o] = pack_rect(r);
@@ -456,29 +475,38 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
     project_stage_kernel<<<grid, 256, 0, st>>>(n, pos, sr, v, xy, z, ell, conic);
 }
 
-template <int DEG>
+template <int DEG, bool BUCKET>
 static void launch_frame_deg(const FrameArgs& a, cudaStream_t st)
 {
     constexpr int NCOEF = DEG >= 0 ? 3 * (DEG + 1) * (DEG + 1) : 0;
     constexpr int smem = NCOEF * 256 * (int)sizeof(float);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(frame_project_kernel<DEG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(frame_project_kernel<DEG, BUCKET>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
         attr = true;
     }
-    frame_project_kernel<DEG><<<(unsigned)a.num_tiles, 256, smem, st>>>(a);
+    frame_project_kernel<DEG, BUCKET><<<(unsigned)a.num_tiles, 256, smem, st>>>(a);
 }
 
-void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st)
+template <bool BUCKET>
+static void launch_frame_mode(const FrameArgs& a, int deg, cudaStream_t st)
+{
+    switch (deg) {
+        case -1: launch_frame_deg<-1, BUCKET>(a, st); break;
+        case 0: launch_frame_deg<0, BUCKET>(a, st); break;
+        case 1: launch_frame_deg<1, BUCKET>(a, st); break;
+        case 2: launch_frame_deg<2, BUCKET>(a, st); break;
+        default: launch_frame_deg<3, BUCKET>(a, st); break;
+    }
+}
+
+void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st, bool bucket)
 {
     if (a.num_tiles == 0) return;
-    switch (deg) {
-        case -1: launch_frame_deg<-1>(a, st); break;
-        case 0: launch_frame_deg<0>(a, st); break;
-        case 1: launch_frame_deg<1>(a, st); break;
-        case 2: launch_frame_deg<2>(a, st); break;
-        default: launch_frame_deg<3>(a, st); break;
-    }
+    if (bucket)
+        launch_frame_mode<true>(a, deg, st);
+    else
+        launch_frame_mode<false>(a, deg, st);
 }
 
 void launch_count_stage(const FrameArgs& a, cudaStream_t st)

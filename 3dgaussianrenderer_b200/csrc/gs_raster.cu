@@ -1,16 +1,17 @@
 // Tile rasteriser (replaces rasterizeTilesKernel, core/gaussian_render.cu:679-775).
 //
 // One CTA per tile, one thread per pixel; each warp owns an 8x4 block of
-// the tile.  The tile's depth-sorted entries are consumed in batches of one
-// entry per thread: every thread gathers one splat (centre, conic + opacity,
-// colour) into shared memory, then the pixels blend the batch front to
-// back in FP32 with the reference's arithmetic.
+// the tile.  The tile's depth-sorted entries are staged in shared memory
+// (centre, conic + opacity, colour) and the pixels blend them front to back
+// in FP32 with the reference's arithmetic.
 //
 // Termination:
 //  * GS_TERM_REFERENCE: every pixel evaluates every entry; after every 32nd
 //    entry of the tile's list the CTA stops once no in-image pixel has
-//    T > 0.02 (the reference's test at :745, at the same granularity
-//    whatever the batch size).  Bit-identical to the reference kernel.
+//    T > 0.02 (the reference's test at :745).  Batches of 32 entries,
+//    double-buffered so the gather of the next batch overlaps the blending
+//    of this one.  Bit-identical to the reference kernel.  (The GS_TERM_TMIN
+//    variant of this kernel stages one entry per thread.)
 //  * GS_TERM_TMIN: a pixel stops once its T < t_min; a warp whose pixels are
 //    all done skips the rest (warp ballot), the CTA stops when every pixel
 //    is done.  Each warp first tests 32 staged splats at a time against its
@@ -49,6 +50,40 @@ __device__ __forceinline__ void blend(const float cx, const float cy, const floa
     T *= (1.0f - alpha);
 }
 
+// Reference-mode blend with the staged conic as stored (a, b, c, 0) and
+// the opacity in the colour's w, as in gaussian_render.cu:727-737.
+__device__ __forceinline__ void blend_ref(const float cx, const float cy, const float2 c, const float4 k,
+                                          const float4 col, float& r, float& g, float& b, float& T)
+{
+    const float dx = cx - c.x, dy = cy - c.y;
+    const float q = k.x * dx * dx + k.z * dy * dy + 2.0f * k.y * dx * dy;
+    const float density = __expf(-0.5f * q);
+    const float alpha = col.w * __saturatef(density);
+    r += col.x * T * alpha;
+    g += col.y * T * alpha;
+    b += col.z * T * alpha;
+    T *= (1.0f - alpha);
+}
+
+__device__ __forceinline__ void cp_async(void* dst, const void* src, const int bytes_is_16)
+{
+    if (bytes_is_16)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+// Copies entry `s` (centre, conic, colour) into shared-memory slot `slot`.
+__device__ __forceinline__ void stage_entry(const RasterArgs& a, const int s, const struct RasterSmem& sm,
+                                            const int slot)
+{
+    cp_async(&sm.xy[slot], &a.xy[s], 0);
+    cp_async(&sm.con[slot], &a.conic[s], 1);
+    cp_async(&sm.col[slot], &a.color[s], 1);
+}
+
 template <int TW, int TH, int MODE>
 __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParams& v, const int64_t gtile,
                                             const int local_tile, const RasterSmem& sm)
@@ -81,7 +116,42 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
     float T = 1.0f;
     bool done = !inimg;
 
-    for (int base = 0; base < count; base += NT) {
+    if (MODE == 0) {
+        // The reference's batches of 32 entries with the tile-wide test after
+        // each, double-buffered: the first warp starts asynchronous copies
+        // (cp.async, global -> shared, no registers held) of batch k + 1 and
+        // loads the indices of batch k + 2 before the tile blends batch k;
+        // the barrier that ends batch k also publishes batch k + 1.
+        const bool loader = threadIdx.x < 32;
+        const int t = (int)threadIdx.x;
+        if (loader && t < count) stage_entry(a, __ldg(&a.values[first + t]), sm, t);
+        cp_async_commit();
+        int idx_next = (loader && 32 + t < count) ? __ldg(&a.values[first + 32 + t]) : 0;
+        cp_async_wait_all();
+        __syncthreads();
+        for (int base = 0; base < count; base += 32) {
+            const int buf = (base >> 5) & 1;
+            const int nb = min(32, count - base);
+            if (loader && base + 32 + t < count) stage_entry(a, idx_next, sm, 32 * (buf ^ 1) + t);
+            cp_async_commit();
+            const int n2 = base + 64 + t;
+            const int idx2 = (loader && n2 < count) ? __ldg(&a.values[first + n2]) : 0;
+            const float2* bxy = sm.xy + 32 * buf;
+            const float4* bcon = sm.con + 32 * buf;
+            const float4* bcol = sm.col + 32 * buf;
+            if (nb == 32) {
+#pragma unroll 8
+                for (int j = 0; j < 32; ++j) blend_ref(cx, cy, bxy[j], bcon[j], bcol[j], r, g, b, T);
+            } else {
+                for (int j = 0; j < nb; ++j) blend_ref(cx, cy, bxy[j], bcon[j], bcol[j], r, g, b, T);
+            }
+            idx_next = idx2;
+            cp_async_wait_all();
+            if (__syncthreads_count(inimg && T > 0.02f) == 0) break;
+        }
+    }
+
+    for (int base = 0; MODE == 1 && base < count; base += NT) {
         const int nb = min(NT, count - base);
         __syncthreads();
         if ((int)threadIdx.x < nb) {
@@ -92,7 +162,7 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
             sm.xy[threadIdx.x] = c;
             sm.con[threadIdx.x] = make_float4(con.x, con.y, con.z, col.w);
             sm.col[threadIdx.x] = col;
-            if (MODE == 1) {
+            {
                 float4 box;
                 const float det = con.x * con.z - con.y * con.y;
                 if (!(col.w > kCullAlpha)) {
@@ -108,20 +178,7 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
             }
         }
         __syncthreads();
-        if (MODE == 0) {
-            bool stop = false;
-            for (int j = 0; j < nb; ++j) {
-                blend(cx, cy, sm.xy[j], sm.con[j], sm.col[j], r, g, b, T);
-                const int e = base + j + 1;
-                if ((e & 31) == 0 || e == count) {
-                    if (__syncthreads_count(inimg && T > 0.02f) == 0) {
-                        stop = true;
-                        break;
-                    }
-                }
-            }
-            if (stop) break;
-        } else {
+        {
             for (int c0 = 0; c0 < nb; c0 += 32) {
                 if (__all_sync(kFull, done)) break;
                 const int j = c0 + lane;
@@ -155,7 +212,7 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
 }
 
 template <int TW, int TH, int MODE>
-__global__ void __launch_bounds__(TW * TH) raster_kernel(RasterArgs a)
+__global__ void __launch_bounds__(TW * TH, 2048 / (TW * TH) * 5 / 8) raster_kernel(RasterArgs a)
 {
     __shared__ float2 s_xy[TW * TH];
     __shared__ float4 s_con[TW * TH];

@@ -70,9 +70,21 @@ typedef struct gs_render_cfg {
     int32_t termination;   /* GS_TERM_REFERENCE (T<=0.02 tile-wide every 32 entries) or GS_TERM_TMIN */
     float t_min;           /* per-pixel transmittance floor for GS_TERM_TMIN (1e-4) */
     int32_t tile_w, tile_h;/* 16x16 (reference), 16x8 or 8x8 */
-    int32_t sort_variant;  /* onesweep tile shape: 0 = 512x8 keys, 1 = 256x8, 2 = 256x16, 3 = 512x16 */
-    int32_t views_per_block; /* views the fused projection handles per block (0 = 8) */
+    int32_t ordering;      /* GS_ORDER_BUCKETS (default) or GS_ORDER_ONESWEEP: how the tile list is ordered */
+    int32_t sort_variant;  /* GS_ORDER_ONESWEEP tile shape: 0 = 512x8 keys, 1 = 256x8, 2 = 256x16, 3 = 512x16 */
+    int32_t views_per_block; /* views the fused projection handles per block (0 = 16) */
+    int32_t graph;         /* 1 (default): a frame whose scene, options and views' sizes and outputs repeat
+                              is captured once into a CUDA graph and replayed; 0: plain stream launches */
 } gs_render_cfg;
+
+/* Tile-list ordering of the whole-frame entry points.  Both give the order of
+ * the reference's stable (tile | depth) sort of keys emitted in Gaussian
+ * order.  BUCKETS: per-tile counts, keys written straight into their tile's
+ * range, one shared-memory depth sort per tile.  ONESWEEP: keys in Gaussian
+ * order, onesweep radix sort on the significant tile and depth bits, then
+ * per-tile ranges (the reference's structure, core/gaussian_render.cu:312-677). */
+#define GS_ORDER_BUCKETS 0
+#define GS_ORDER_ONESWEEP 1
 
 /* Per-stage device times of one frame, same fields as the reference's
  * RenderStats (core/types.h:26-33), plus the tile-list size. */
@@ -81,6 +93,8 @@ typedef struct gs_stats {
     int64_t num_keys;
     int64_t num_tiles;
     int64_t kernel_launches; /* gs_b200 kernels launched for the frame */
+    int32_t graph_replay;    /* 1: the frame ran as a replay of a captured CUDA graph */
+    int32_t attempts;        /* launches of the frame: 2 when the tile list outgrew its buffers and was redone */
 } gs_stats;
 
 typedef struct gs_ctx gs_ctx;
