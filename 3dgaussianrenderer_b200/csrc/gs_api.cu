@@ -92,6 +92,7 @@ struct Counters {
     unsigned long long slots;                      // (view, Gaussian) slots taken by the frame kernel
     int64_t total;                                 // K
     int64_t sort_n;                                // min(K, key capacity)
+    unsigned int mid_tiles, big_tiles;             // tiles for the CTA sorts
     int err;
     int overflow;                                  // K > key capacity: the frame must be redone
     uint32_t epoch_scan, epoch_sort;               // look-back epochs of this frame
@@ -138,7 +139,7 @@ struct gs_ctx {
     DevBuf keys0, vals0, keys1, vals1;     // tile lists
     DevBuf sort_hist, sort_status;
     DevBuf ranges;
-    DevBuf tile_count, cursor;             // tile-bucket ordering: keys per tile, bucket fill cursors
+    DevBuf tile_count, cursor, big_list;   // tile-bucket ordering: keys per tile, bucket fill cursors, big tiles
     DevBuf counters;
     DevBuf image;                          // images of the host-output variants
     Counters* h_counters = nullptr;        // pinned mirror
@@ -514,7 +515,7 @@ int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams,
         if (ctx->scan_status.ensure(sizeof(uint64_t) * scan_blocks, true)) return fail(GS_ERR_OOM, "scan status");
     }
     if (ctx->ranges.ensure(sizeof(int32_t) * 2 * tiles) || ctx->tile_count.ensure(sizeof(uint32_t) * tiles) ||
-        ctx->cursor.ensure(sizeof(unsigned long long) * tiles))
+        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(2 * sizeof(int32_t) * tiles))
         return fail(GS_ERR_OOM, "tile buffers");
     return GS_OK;
 }
@@ -573,6 +574,10 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ta.capacity = ctx->key_capacity;
     ta.sort_n = &dc->sort_n;
     ta.overflow = &dc->overflow;
+    ta.mid_list = ctx->big_list.as<int32_t>();
+    ta.mid_count = &dc->mid_tiles;
+    ta.big_list = ctx->big_list.as<int32_t>() + std::max<int64_t>(p.tiles_total, 1);
+    ta.big_count = &dc->big_tiles;
     launch_tile_scan(ta, st);
     GS_CUDA(record(ctx->ev[1], st, capturing));
     GS_CUDA(record(ctx->ev[2], st, capturing));
@@ -602,7 +607,11 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     sa.vals = ctx->vals0.as<int32_t>();
     sa.vals_alt = ctx->vals1.as<int32_t>();
     sa.slot_gi = ctx->offsets.as<int32_t>();
-    if (p.n > 0) launch_tile_sort(sa, st);
+    sa.mid_list = ctx->big_list.as<int32_t>();
+    sa.mid_count = &dc->mid_tiles;
+    sa.big_list = ctx->big_list.as<int32_t>() + std::max<int64_t>(p.tiles_total, 1);
+    sa.big_count = &dc->big_tiles;
+    if (p.n > 0) launch_tile_sort(sa, ctx->num_sms, st);
     GS_CUDA(record(ctx->ev[4], st, capturing));
 
     RasterArgs ra{};
@@ -631,7 +640,7 @@ uint64_t layout_of(const gs_ctx* ctx)
 {
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                             &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->keys0, &ctx->vals0,
-                            &ctx->keys1, &ctx->vals1, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->counters};
+                            &ctx->keys1, &ctx->vals1, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->counters};
     uint64_t h = 1469598103934665603ull;
     auto mix = [&h](uint64_t x) { h = (h ^ x) * 1099511628211ull; };
     for (const DevBuf* b : bufs) {
@@ -767,8 +776,8 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
         stats->num_keys = ctx->h_counters->total;
         stats->num_tiles = p.tiles_total;
-        // frame kernel, tile scan, bucket emit, tile sort, raster
-        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 2;
+        // frame kernel, tile scan, bucket emit, tile sorts (warp, mid, big), raster
+        stats->kernel_launches = (p.n > 0 ? 5 : 0) + 2;
         stats->graph_replay = replayed ? 1 : 0;
         stats->attempts = attempts;
     }
@@ -905,7 +914,7 @@ int gs_ctx_destroy(gs_ctx* ctx)
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                       &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
-                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->counters, &ctx->image};
+                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->counters, &ctx->image};
     for (DevBuf* b : bufs) b->release();
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_init) cudaFreeHost(ctx->h_init);
@@ -921,7 +930,7 @@ int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
     if (!ctx) return 0;
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                             &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
-                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->counters, &ctx->image};
+                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->counters, &ctx->image};
     int64_t t = 0;
     for (const DevBuf* b : bufs) t += (int64_t)b->bytes;
     return t;

@@ -88,6 +88,10 @@ struct TileScanArgs {
     int64_t capacity;
     int64_t* sort_n;                 // min(K, capacity)
     int* overflow;                   // K > capacity
+    int32_t* mid_list;               // out: tiles with kWarpTile < keys <= kMidTile
+    unsigned int* mid_count;
+    int32_t* big_list;               // out: tiles with more than kMidTile keys
+    unsigned int* big_count;
 };
 
 // Per-tile sort of the buckets: each tile's keys are ordered by depth and,
@@ -101,8 +105,14 @@ struct TileSortArgs {
     int32_t* vals;                   // out: slots in blend order
     int32_t* vals_alt;
     const int32_t* slot_gi;
+    int32_t* mid_list;               // tiles for the CTA sort (from the tile scan, plus warp-sort ties)
+    unsigned int* mid_count;
+    const int32_t* big_list;         // tiles above kMidTile keys (from the tile scan)
+    const unsigned int* big_count;
 };
 constexpr int kTileSortSmemKeys = 4096;
+constexpr int kWarpTile = 256;       // tiles up to this many keys are sorted by one warp
+constexpr int kMidTile = 1024;       // ... up to this many by one high-occupancy CTA
 constexpr int kTileScanItems = 4096;  // tiles per scan block
 
 struct EmitArgs {
@@ -170,7 +180,7 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
 void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st, bool bucket = false);
 void launch_tile_scan(const TileScanArgs& a, cudaStream_t st);
 void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st);
-void launch_tile_sort(const TileSortArgs& a, cudaStream_t st);
+void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st);
 void launch_count_stage(const FrameArgs& a, cudaStream_t st);
 // view_base[v] = sum of view_total[u < v]; *total = sum of all.  With a
 // non-null `sort_n`, also *sort_n = min(total, capacity) and *overflow = 1

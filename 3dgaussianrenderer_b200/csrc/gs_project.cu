@@ -188,6 +188,7 @@ __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
 }
 
 // ---- fused frame kernel ------------------------------------------------------
+
 //
 // Block `tile` (taken in dynamic order, so a look-back only ever waits on a
 // block that is already running) owns group g = tile % groups for views

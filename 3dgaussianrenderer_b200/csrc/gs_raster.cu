@@ -116,41 +116,6 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
     float T = 1.0f;
     bool done = !inimg;
 
-    if (MODE == 0) {
-        // The reference's batches of 32 entries with the tile-wide test after
-        // each, double-buffered: the first warp starts asynchronous copies
-        // (cp.async, global -> shared, no registers held) of batch k + 1 and
-        // loads the indices of batch k + 2 before the tile blends batch k;
-        // the barrier that ends batch k also publishes batch k + 1.
-        const bool loader = threadIdx.x < 32;
-        const int t = (int)threadIdx.x;
-        if (loader && t < count) stage_entry(a, __ldg(&a.values[first + t]), sm, t);
-        cp_async_commit();
-        int idx_next = (loader && 32 + t < count) ? __ldg(&a.values[first + 32 + t]) : 0;
-        cp_async_wait_all();
-        __syncthreads();
-        for (int base = 0; base < count; base += 32) {
-            const int buf = (base >> 5) & 1;
-            const int nb = min(32, count - base);
-            if (loader && base + 32 + t < count) stage_entry(a, idx_next, sm, 32 * (buf ^ 1) + t);
-            cp_async_commit();
-            const int n2 = base + 64 + t;
-            const int idx2 = (loader && n2 < count) ? __ldg(&a.values[first + n2]) : 0;
-            const float2* bxy = sm.xy + 32 * buf;
-            const float4* bcon = sm.con + 32 * buf;
-            const float4* bcol = sm.col + 32 * buf;
-            if (nb == 32) {
-#pragma unroll 8
-                for (int j = 0; j < 32; ++j) blend_ref(cx, cy, bxy[j], bcon[j], bcol[j], r, g, b, T);
-            } else {
-                for (int j = 0; j < nb; ++j) blend_ref(cx, cy, bxy[j], bcon[j], bcol[j], r, g, b, T);
-            }
-            idx_next = idx2;
-            cp_async_wait_all();
-            if (__syncthreads_count(inimg && T > 0.02f) == 0) break;
-        }
-    }
-
     for (int base = 0; MODE == 1 && base < count; base += NT) {
         const int nb = min(NT, count - base);
         __syncthreads();
@@ -211,13 +176,139 @@ __device__ __forceinline__ void raster_tile(const RasterArgs& a, const ViewParam
     }
 }
 
+__device__ __forceinline__ void store_pixel(const ViewParams& v, const int px, const int py, const float r,
+                                            const float g, const float b)
+{
+    uchar4 qc;
+    qc.x = r * 255;
+    qc.y = g * 255;
+    qc.z = b * 255;
+    qc.w = 255;
+    v.out[(int64_t)py * v.width + px] = qc;
+}
+
+// ---- GS_TERM_REFERENCE ------------------------------------------------------------
+//
+// The reference's blend and termination, bit for bit: every pixel evaluates
+// every entry, in batches of 32, and after each batch the tile stops once no
+// pixel has T > 0.02.  Each warp owns an 8x8 pixel block, two pixels per
+// thread (rows y and y + 4), so the staged entry is read from shared memory
+// once for two blends.  The batches are double-buffered: the first warp
+// starts asynchronous copies (cp.async, global -> shared, no registers held)
+// of batch k + 1 and loads the indices of batch k + 2 before the tile blends
+// batch k; the barrier that ends batch k also publishes batch k + 1.
+struct RefSmem {
+    float2 xy[64];
+    float4 con[64];
+    float4 col[64];
+};
+
+template <int TW, int TH>
+__device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewParams& v, const int64_t gtile,
+                                                const int local_tile, RefSmem& sm)
+{
+    constexpr int WX = TW / 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int first = __ldg(&a.ranges[2 * gtile]);
+    const int last = __ldg(&a.ranges[2 * gtile + 1]);
+    const int count = last - first;
+    const int tx = local_tile % v.tiles_x, ty = local_tile / v.tiles_x;
+    const int wx0 = tx * TW + (warp % WX) * 8, wy0 = ty * TH + (warp / WX) * 8;
+    const int px = wx0 + (lane & 7), py0 = wy0 + (lane >> 3), py1 = py0 + 4;
+    const bool in0 = px < v.width && py0 < v.height;
+    const bool in1 = px < v.width && py1 < v.height;
+    if (count <= 0) {
+        // the reference clears the image and skips empty tiles (main.cpp:363);
+        // writing zeros here instead saves the separate clear
+        if (a.write_empty) {
+            if (in0) v.out[(int64_t)py0 * v.width + px] = make_uchar4(0, 0, 0, 0);
+            if (in1) v.out[(int64_t)py1 * v.width + px] = make_uchar4(0, 0, 0, 0);
+        }
+        return;
+    }
+    // pixel corner sample, gaussian_render.cu:701-704
+    const float cx = (float)px * v.texel_x - 1.0f;
+    const float cy0 = (float)py0 * v.texel_y - 1.0f;
+    const float cy1 = (float)py1 * v.texel_y - 1.0f;
+    float r0 = 0.0f, g0 = 0.0f, b0 = 0.0f, T0 = 1.0f;
+    float r1 = 0.0f, g1 = 0.0f, b1 = 0.0f, T1 = 1.0f;
+    const RasterSmem rs = {sm.xy, sm.con, sm.col, nullptr};
+    const bool loader = threadIdx.x < 32;
+    const int t = (int)threadIdx.x;
+    if (loader && t < count) stage_entry(a, __ldg(&a.values[first + t]), rs, t);
+    cp_async_commit();
+    int idx_next = (loader && 32 + t < count) ? __ldg(&a.values[first + 32 + t]) : 0;
+    cp_async_wait_all();
+    __syncthreads();
+    for (int base = 0; base < count; base += 32) {
+        const int buf = (base >> 5) & 1;
+        const int nb = min(32, count - base);
+        if (loader && base + 32 + t < count) stage_entry(a, idx_next, rs, 32 * (buf ^ 1) + t);
+        cp_async_commit();
+        const int n2 = base + 64 + t;
+        const int idx2 = (loader && n2 < count) ? __ldg(&a.values[first + n2]) : 0;
+        const float2* bxy = sm.xy + 32 * buf;
+        const float4* bcon = sm.con + 32 * buf;
+        const float4* bcol = sm.col + 32 * buf;
+        if (nb == 32) {
+#pragma unroll 4
+            for (int j = 0; j < 32; ++j) {
+                blend_ref(cx, cy0, bxy[j], bcon[j], bcol[j], r0, g0, b0, T0);
+                blend_ref(cx, cy1, bxy[j], bcon[j], bcol[j], r1, g1, b1, T1);
+            }
+        } else {
+            for (int j = 0; j < nb; ++j) {
+                blend_ref(cx, cy0, bxy[j], bcon[j], bcol[j], r0, g0, b0, T0);
+                blend_ref(cx, cy1, bxy[j], bcon[j], bcol[j], r1, g1, b1, T1);
+            }
+        }
+        idx_next = idx2;
+        cp_async_wait_all();
+        if (__syncthreads_count((in0 && T0 > 0.02f) || (in1 && T1 > 0.02f)) == 0) break;
+    }
+    if (in0) store_pixel(v, px, py0, r0, g0, b0);
+    if (in1) store_pixel(v, px, py1, r1, g1, b1);
+}
+
+template <int TW, int TH>
+__global__ void __launch_bounds__(TW * TH / 2) raster_ref_kernel(RasterArgs a)
+{
+    __shared__ RefSmem sm;
+    raster_ref_tile<TW, TH>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, sm);
+}
+
+// Persistent variant over the flattened tiles of all views.
+template <int TW, int TH>
+__global__ void __launch_bounds__(TW * TH / 2) raster_ref_persistent_kernel(RasterArgs a)
+{
+    __shared__ RefSmem sm;
+    __shared__ int64_t s_tile;
+    for (;;) {
+        __syncthreads();
+        if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(a.tile_counter, 1ull);
+        __syncthreads();
+        const int64_t gtile = s_tile;
+        if (gtile >= a.num_tiles_total) return;
+        int lo = 0, hi = a.num_views - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (a.views[mid].tile_offset <= gtile)
+                lo = mid;
+            else
+                hi = mid - 1;
+        }
+        const ViewParams& v = a.views[lo];
+        raster_ref_tile<TW, TH>(a, v, gtile, (int)(gtile - v.tile_offset), sm);
+    }
+}
+
 template <int TW, int TH, int MODE>
 __global__ void __launch_bounds__(TW * TH, 2048 / (TW * TH) * 5 / 8) raster_kernel(RasterArgs a)
 {
     __shared__ float2 s_xy[TW * TH];
     __shared__ float4 s_con[TW * TH];
     __shared__ float4 s_col[TW * TH];
-    __shared__ float4 s_box[MODE == 1 ? TW * TH : 1];
+    __shared__ float4 s_box[TW * TH];
     const RasterSmem sm = {s_xy, s_con, s_col, s_box};
     raster_tile<TW, TH, MODE>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, sm);
 }
@@ -229,7 +320,7 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
     __shared__ float2 s_xy[TW * TH];
     __shared__ float4 s_con[TW * TH];
     __shared__ float4 s_col[TW * TH];
-    __shared__ float4 s_box[MODE == 1 ? TW * TH : 1];
+    __shared__ float4 s_box[TW * TH];
     __shared__ int64_t s_tile;
     const RasterSmem sm = {s_xy, s_con, s_col, s_box};
     for (;;) {
@@ -255,12 +346,15 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
 // ---- GS_TERM_TMIN from raster records --------------------------------------
 //
 // The frame pipeline's kernel for the T_min mode.  One CTA per tile (all
-// views' tiles in one grid), but no CTA-wide barrier: each warp walks the
-// tile's sorted list on its own, 32 entries at a time -- lane l loads entry
-// l's record (48 bytes, gathered through L1, shared by the tile's warps),
-// tests its cull extents against the warp's 8x4 pixel block, and the warp
-// blends the survivors in list order, each broadcast from a per-warp
-// shared-memory slot.  A warp stops when all its pixels have T < t_min.
+// views' tiles in one grid), no CTA-wide barrier: each warp owns an 8x8
+// pixel block, two pixels per lane (rows y and y + 4, same column), and
+// walks the tile's sorted list on its own, 32 entries at a time -- lane l
+// loads entry l's record (48 bytes, gathered through L1, shared by the
+// tile's warps) and tests its cull extents against the block; the
+// survivors are packed in list order into per-warp shared-memory slots
+// (rank = popcount of the ballot below the lane) and every lane blends them
+// into both its pixels.  The column offset terms of the exponent are shared
+// by the two pixels.  A warp stops when all its pixels have T < t_min.
 // Blend per pixel: p = A dx^2 + B dx dy + C dy^2, alpha = opacity * 2^p,
 // w = T alpha, colour += rgb w, T -= w.
 
@@ -271,12 +365,28 @@ __device__ __forceinline__ float ex2_approx(const float x)
     return y;
 }
 
-template <int TW, int TH>
-__global__ void __launch_bounds__(TW * TH) raster_rec_kernel(RasterArgs a)
+__device__ __forceinline__ void blend_rec(const float dy, const float adx2, const float bdx, const float4 e1,
+                                          const float eb, float& r, float& g, float& b, float& T, bool& done,
+                                          const float tmin)
 {
-    constexpr int NW = TW * TH / 32;
+    const float p = fmaf(fmaf(e1.x, dy, bdx), dy, adx2);
+    const float w = T * (e1.y * ex2_approx(p));
+    r = fmaf(e1.z, w, r);
+    g = fmaf(e1.w, w, g);
+    b = fmaf(eb, w, b);
+    T -= w;
+    done = T < tmin;
+}
+
+
+template <int TW, int TH>
+__global__ void __launch_bounds__(TW * TH / 2) raster_rec_kernel(RasterArgs a)
+{
+    constexpr int NW = TW * TH / 64;
     constexpr int WX = TW / 8;
-    __shared__ float4 s_slot[NW][3][32];
+    __shared__ float4 s_q0[NW][32];
+    __shared__ float4 s_q1[NW][32];
+    __shared__ float s_qb[NW][32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t gtile = blockIdx.x;
     int vi = 0;
@@ -295,73 +405,83 @@ __global__ void __launch_bounds__(TW * TH) raster_rec_kernel(RasterArgs a)
     const int first = __ldg(&a.ranges[2 * gtile]);
     const int last = __ldg(&a.ranges[2 * gtile + 1]);
     const int tx = local_tile % v.tiles_x, ty = local_tile / v.tiles_x;
-    const int wx0 = tx * TW + (warp % WX) * 8, wy0 = ty * TH + (warp / WX) * 4;
-    const int px = wx0 + (lane & 7), py = wy0 + (lane >> 3);
-    const bool inimg = px < v.width && py < v.height;
+    const int wx0 = tx * TW + (warp % WX) * 8, wy0 = ty * TH + (warp / WX) * 8;
+    const int px = wx0 + (lane & 7), py0 = wy0 + (lane >> 3), py1 = py0 + 4;
+    const bool in0 = px < v.width && py0 < v.height;
+    const bool in1 = px < v.width && py1 < v.height;
     if (last - first <= 0) {
-        if (a.write_empty && inimg) v.out[(int64_t)py * v.width + px] = make_uchar4(0, 0, 0, 0);
+        if (a.write_empty) {
+            if (in0) v.out[(int64_t)py0 * v.width + px] = make_uchar4(0, 0, 0, 0);
+            if (in1) v.out[(int64_t)py1 * v.width + px] = make_uchar4(0, 0, 0, 0);
+        }
         return;
     }
     const float cx = (float)px * v.texel_x - 1.0f;
-    const float cy = (float)py * v.texel_y - 1.0f;
+    const float cy0 = (float)py0 * v.texel_y - 1.0f;
+    const float cy1 = (float)py1 * v.texel_y - 1.0f;
     const float bx0 = (float)wx0 * v.texel_x - 1.0f, bx1 = (float)(wx0 + 7) * v.texel_x - 1.0f;
-    const float by0 = (float)wy0 * v.texel_y - 1.0f, by1 = (float)(wy0 + 3) * v.texel_y - 1.0f;
-    float r = 0.0f, g = 0.0f, b = 0.0f, T = 1.0f;
-    bool done = !inimg;
+    const float by0 = (float)wy0 * v.texel_y - 1.0f, by1 = (float)(wy0 + 7) * v.texel_y - 1.0f;
+    float r0 = 0.0f, g0 = 0.0f, b0 = 0.0f, T0 = 1.0f;
+    float r1 = 0.0f, g1 = 0.0f, b1 = 0.0f, T1 = 1.0f;
+    bool d0 = !in0, d1 = !in1;
     const float tmin = a.t_min;
+    const unsigned lt = lanemask_lt();
 
     for (int base = first; base < last; base += 32) {
-        if (__all_sync(kFull, done)) break;
+        if (__all_sync(kFull, d0 && d1)) break;
         const int j = base + lane;
         bool keep = false;
+        float4 q0, q2;
+        const float4* rp = nullptr;
         if (j < last) {
             const int s = __ldg(&a.values[j]);
-            const float4* rp = a.rec + 3 * (int64_t)s;
-            const float4 r0 = __ldg(rp), r2 = __ldg(rp + 2);
-            keep = (r0.x - r2.y <= bx1) && (r0.x + r2.y >= bx0) && (r0.y - r2.z <= by1) && (r0.y + r2.z >= by0);
-            if (keep) {
-                s_slot[warp][0][lane] = r0;
-                s_slot[warp][1][lane] = __ldg(rp + 1);
-                s_slot[warp][2][lane] = r2;
-            }
+            rp = a.rec + 3 * (int64_t)s;
+            q0 = __ldg(rp);
+            q2 = __ldg(rp + 2);
+            keep = (q0.x - q2.y <= bx1) && (q0.x + q2.y >= bx0) && (q0.y - q2.z <= by1) && (q0.y + q2.z >= by0);
         }
-        unsigned m = __ballot_sync(kFull, keep);
+        const unsigned bal = __ballot_sync(kFull, keep);
+        if (keep) {
+            const int k = __popc(bal & lt);
+            s_q0[warp][k] = q0;
+            s_q1[warp][k] = __ldg(rp + 1);
+            s_qb[warp][k] = q2.x;
+        }
         __syncwarp();  // slot writes visible to the whole warp
-        while (m) {
-            const int k = __ffs(m) - 1;
-            m &= m - 1;
-            const float4 q0 = s_slot[warp][0][k];
-            const float4 q1 = s_slot[warp][1][k];
-            const float qb = s_slot[warp][2][k].x;
-            if (!done) {
-                const float dx = cx - q0.x, dy = cy - q0.y;
-                const float p = fmaf(fmaf(q0.z, dx, q0.w * dy), dx, q1.x * dy * dy);
-                const float alpha = q1.y * ex2_approx(p);
-                const float w = T * alpha;
-                r = fmaf(q1.z, w, r);
-                g = fmaf(q1.w, w, g);
-                b = fmaf(qb, w, b);
-                T -= w;
-                done = T < tmin;
-            }
+        const int cnt = __popc(bal);
+        for (int k = 0; k < cnt; ++k) {
+            const float4 e0 = s_q0[warp][k];
+            const float4 e1 = s_q1[warp][k];
+            const float eb = s_qb[warp][k];
+            const float dx = cx - e0.x;
+            const float adx2 = e0.z * dx * dx;
+            const float bdx = e0.w * dx;
+            if (!d0) blend_rec(cy0 - e0.y, adx2, bdx, e1, eb, r0, g0, b0, T0, d0, tmin);
+            if (!d1) blend_rec(cy1 - e0.y, adx2, bdx, e1, eb, r1, g1, b1, T1, d1, tmin);
         }
         __syncwarp();  // slots are rewritten by the next chunk
     }
-    if (inimg) {
-        uchar4 qc;
-        qc.x = r * 255;
-        qc.y = g * 255;
-        qc.z = b * 255;
-        qc.w = 255;
-        v.out[(int64_t)py * v.width + px] = qc;
-    }
+    if (in0) store_pixel(v, px, py0, r0, g0, b0);
+    if (in1) store_pixel(v, px, py1, r1, g1, b1);
 }
 
 template <int TW, int TH>
 static void launch_shape(const RasterArgs& a, int termination, bool persistent, int num_sms, cudaStream_t st)
 {
     if (a.rec && termination == 1) {
-        if (a.num_tiles_total > 0) raster_rec_kernel<TW, TH><<<(unsigned)a.num_tiles_total, TW * TH, 0, st>>>(a);
+        if (a.num_tiles_total > 0) raster_rec_kernel<TW, TH><<<(unsigned)a.num_tiles_total, TW * TH / 2, 0, st>>>(a);
+        return;
+    }
+    if (termination == 0) {
+        if (a.num_tiles_total <= 0) return;
+        if (persistent) {
+            int per_sm = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, raster_ref_persistent_kernel<TW, TH>, TW * TH / 2, 0);
+            const int64_t grid = std::min<int64_t>((int64_t)std::max(per_sm, 1) * num_sms, a.num_tiles_total);
+            raster_ref_persistent_kernel<TW, TH><<<(unsigned)grid, TW * TH / 2, 0, st>>>(a);
+        } else {
+            raster_ref_kernel<TW, TH><<<(unsigned)a.num_tiles_total, TW * TH / 2, 0, st>>>(a);
+        }
         return;
     }
     if (persistent) {
