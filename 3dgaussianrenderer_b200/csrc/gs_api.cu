@@ -92,7 +92,7 @@ struct Counters {
     unsigned long long slots;                      // (view, Gaussian) slots taken by the frame kernel
     int64_t total;                                 // K
     int64_t sort_n;                                // min(K, key capacity)
-    unsigned int mid_tiles, big_tiles;             // tiles for the CTA sorts
+    unsigned int big_tiles;                        // tiles sorted ahead of the raster
     int err;
     int overflow;                                  // K > key capacity: the frame must be redone
     uint32_t epoch_scan, epoch_sort;               // look-back epochs of this frame
@@ -422,7 +422,7 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     // 4. tile ranges + raster
     GS_CUDA(cudaMemsetAsync(ctx->ranges.p, 0xFF, sizeof(int32_t) * 2 * (size_t)tiles_total, st));
     if (K > 0) launch_ranges(skeys, K, nullptr, ctx->ranges.as<int32_t>(), st);
-    RasterArgs ra;
+    RasterArgs ra{};
     ra.view0 = ctx->h_views[0];
     ra.views = ctx->views.as<ViewParams>();
     ra.num_views = num_views;
@@ -515,7 +515,7 @@ int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams,
         if (ctx->scan_status.ensure(sizeof(uint64_t) * scan_blocks, true)) return fail(GS_ERR_OOM, "scan status");
     }
     if (ctx->ranges.ensure(sizeof(int32_t) * 2 * tiles) || ctx->tile_count.ensure(sizeof(uint32_t) * tiles) ||
-        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(2 * sizeof(int32_t) * tiles))
+        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(sizeof(int32_t) * tiles))
         return fail(GS_ERR_OOM, "tile buffers");
     return GS_OK;
 }
@@ -574,10 +574,9 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ta.capacity = ctx->key_capacity;
     ta.sort_n = &dc->sort_n;
     ta.overflow = &dc->overflow;
-    ta.mid_list = ctx->big_list.as<int32_t>();
-    ta.mid_count = &dc->mid_tiles;
-    ta.big_list = ctx->big_list.as<int32_t>() + std::max<int64_t>(p.tiles_total, 1);
+    ta.big_list = ctx->big_list.as<int32_t>();
     ta.big_count = &dc->big_tiles;
+    ta.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     launch_tile_scan(ta, st);
     GS_CUDA(record(ctx->ev[1], st, capturing));
     GS_CUDA(record(ctx->ev[2], st, capturing));
@@ -607,9 +606,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     sa.vals = ctx->vals0.as<int32_t>();
     sa.vals_alt = ctx->vals1.as<int32_t>();
     sa.slot_gi = ctx->offsets.as<int32_t>();
-    sa.mid_list = ctx->big_list.as<int32_t>();
-    sa.mid_count = &dc->mid_tiles;
-    sa.big_list = ctx->big_list.as<int32_t>() + std::max<int64_t>(p.tiles_total, 1);
+    sa.big_list = ctx->big_list.as<int32_t>();
     sa.big_count = &dc->big_tiles;
     if (p.n > 0) launch_tile_sort(sa, ctx->num_sms, st);
     GS_CUDA(record(ctx->ev[4], st, capturing));
@@ -628,6 +625,9 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ra.rec = cfg.termination == GS_TERM_TMIN ? ctx->rec.as<float4>() : nullptr;
     ra.t_min = cfg.t_min;
     ra.tile_counter = &dc->raster_tile;
+    ra.keys = ctx->keys0.as<uint64_t>();  // tiles up to the fused capacity are sorted by the raster CTA
+    ra.slot_gi = ctx->offsets.as<int32_t>();
+    ra.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, p.num_views > 1, ctx->num_sms, st);
     GS_CUDA(cudaGetLastError());
     GS_CUDA(record(ctx->ev[5], st, capturing));
@@ -776,8 +776,8 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
         stats->num_keys = ctx->h_counters->total;
         stats->num_tiles = p.tiles_total;
-        // frame kernel, tile scan, bucket emit, tile sorts (warp, mid, big), raster
-        stats->kernel_launches = (p.n > 0 ? 5 : 0) + 2;
+        // frame kernel, tile scan, bucket emit, big-tile sort, raster (sorts the other tiles)
+        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 2;
         stats->graph_replay = replayed ? 1 : 0;
         stats->attempts = attempts;
     }

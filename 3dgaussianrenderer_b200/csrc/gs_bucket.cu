@@ -9,15 +9,17 @@
 //   2. bucket emit -- every overlap is written straight into its tile's
 //                     range, at a position claimed with one atomic, as
 //                     (depth << 32 | slot);
-//   3. tile sort   -- one CTA per tile orders the tile's keys by depth in
-//                     shared memory (LSD radix over only the depth bits that
-//                     vary inside the tile), then, if two keys of the tile
-//                     share a depth, re-sorts on (depth, view * n + i).
+//   3. tile sort   -- each tile's keys are ordered by depth in shared
+//                     memory (LSD radix over only the depth bits that vary
+//                     inside the tile), equal depths by view * n + i; small
+//                     tiles by the raster CTA right before it blends them,
+//                     larger ones by a separate kernel.
 // The result per tile is exactly the order of a stable sort of the
 // reference's keys emitted in Gaussian order: depth first, index among equal
 // depths.  Each key crosses HBM about three times (emit, sort read, sorted
 // index write) instead of twice per radix pass.
 #include "gs_kernels.h"
+#include "gs_tilesort.cuh"
 
 #include <algorithm>
 
@@ -126,10 +128,7 @@ __global__ void __launch_bounds__(kThreads) tile_scan_kernel(TileScanArgs a)
     for (int j = 0; j < IPT; ++j) {
         const int64_t t = first + j;
         if (t < a.tiles) {
-            if (c[j] > (uint32_t)kMidTile)
-                a.big_list[atomicAdd(a.big_count, 1u)] = (int32_t)t;
-            else if (c[j] > (uint32_t)kWarpTile)
-                a.mid_list[atomicAdd(a.mid_count, 1u)] = (int32_t)t;
+            if (c[j] > (uint32_t)a.fused_cap) a.big_list[atomicAdd(a.big_count, 1u)] = (int32_t)t;
             a.cursor[t] = (unsigned long long)run;
             const int64_t lo = run < cap ? run : cap;
             const int64_t hi = run + c[j] < cap ? run + c[j] : cap;
@@ -246,202 +245,23 @@ void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st)
     emit_bucket_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(a);
 }
 
-// ---- 3. tile sort ---------------------------------------------------------------
+// ---- 3. sort of the tiles too large for the raster CTAs -------------------------------
+//
+// Tiles up to the fused capacity are sorted by the raster CTA itself
+// (gs_tilesort.cuh).  The larger ones, listed by the tile scan, are sorted
+// here beforehand -- in shared memory up to kTileSortSmemKeys keys, else by
+// stable LSD passes through global memory -- and their order is written to
+// `vals` for the rasteriser to read.
 
 namespace {
 
-struct SortSmem {
-    uint64_t* k;       // [kTileSortSmemKeys]; the warp histograms alias it while ranking
-    int32_t* v;        // [kTileSortSmemKeys]
-    uint32_t* whist;   // [kWarps][256] (aliases k)
-    int32_t* bexcl;    // [256] digit start inside the ranked chunk
-    int32_t* dcount;   // [256] digit count of the ranked chunk
-    int64_t* scan;     // [kWarps]
-    uint64_t* red;     // [2 * kWarps]
-    int32_t* run;      // [256] running digit start (global-memory passes)
-};
-
-// Stable rank of IPT keys per thread by the digit (key >> shift) & 0xFF.
-// Item order: p = warp * 32 * IPT + i * 32 + lane.  pos[i] = rank of item i
-// in the chunk; sm.bexcl / sm.dcount hold each digit's start and count.
-// Every thread must call it; it ends with a barrier.
-template <int IPT>
-__device__ __forceinline__ void block_rank(const uint64_t (&key)[IPT], const int shift, int (&pos)[IPT],
-                                           const SortSmem& sm)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint32_t* wh = sm.whist + warp * 256;
-#pragma unroll
-    for (int k = 0; k < 8; ++k) wh[lane + 32 * k] = 0;
-    __syncwarp();
-    const unsigned lt = lanemask_lt();
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const unsigned d = (unsigned)(key[i] >> shift) & 0xFFu;
-        const unsigned peers = __match_any_sync(kFull, d);
-        const uint32_t before = wh[d];
-        const int below = __popc(peers & lt);
-        __syncwarp();
-        if (below == 0) wh[d] = before + __popc(peers);
-        __syncwarp();
-        pos[i] = (int)before + below;
-    }
-    __syncthreads();
-    const int d = threadIdx.x;  // 256 threads = 256 digits
-    int run = 0;
-#pragma unroll
-    for (int w = 0; w < kWarps; ++w) {
-        const uint32_t c = sm.whist[w * 256 + d];
-        sm.whist[w * 256 + d] = (uint32_t)run;
-        run += (int)c;
-    }
-    const int ex = (int)excl_scan_block((int64_t)run, sm.scan);
-    sm.bexcl[d] = ex;
-    sm.dcount[d] = run;
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const unsigned dd = (unsigned)(key[i] >> shift) & 0xFFu;
-        pos[i] += sm.bexcl[dd] + (int)sm.whist[warp * 256 + dd];
-    }
-    __syncthreads();  // whist (aliasing k) may be overwritten from here on
-}
-
-// LSD passes over the 8-bit windows that cover `mask`, lowest first; the
-// data lives in registers (p order) and goes through shared memory between
-// passes.  Returns with registers and sm.k / sm.v in sorted p order when at
-// least one pass ran.
-template <int IPT>
-__device__ __forceinline__ bool smem_sort(uint64_t (&k)[IPT], int32_t (&v)[IPT], uint64_t mask, const SortSmem& sm)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    bool any = false;
-    while (mask) {
-        const int shift = __ffsll((long long)mask) - 1;
-        mask &= ~(0xFFull << shift);
-        int pos[IPT];
-        block_rank<IPT>(k, shift, pos, sm);
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            sm.k[pos[i]] = k[i];
-            sm.v[pos[i]] = v[i];
-        }
-        __syncthreads();
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const int p = warp * 32 * IPT + i * 32 + lane;
-            k[i] = sm.k[p];
-            v[i] = sm.v[p];
-        }
-        __syncthreads();
-        any = true;
-    }
-    return any;
-}
-
-// Equal depths are common (the depth key has float resolution), so after
-// the depth passes every run of equal depths is put in (view * n + i) order
-// by the thread owning its first item: an insertion sort through the
-// slot -> index table, on runs of at most kMaxTieRun items.  Returns false
-// (nothing changed) when a longer run exists.
-constexpr int kMaxTieRun = 32;
-
-__device__ __forceinline__ uint32_t depth_of(const uint64_t key) { return (uint32_t)(key >> 32); }
-
-// Fixes the tie runs starting at this thread's items of `keys` (sorted by
-// depth; slot in the low 32 bits).  Returns true when a run is too long.
-template <int IPT, int STRIDE>
-__device__ __forceinline__ bool fix_tie_runs(uint64_t* keys, const int m, const int first_p,
-                                             const int32_t* __restrict__ slot_gi)
-{
-    bool too_long = false;
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const int p = first_p + i * STRIDE;
-        if (p >= m) continue;
-        const uint32_t d = depth_of(keys[p]);
-        if ((p > 0 && depth_of(keys[p - 1]) == d) || p + 1 >= m || depth_of(keys[p + 1]) != d) continue;
-        int len = 2;
-        while (p + len < m && depth_of(keys[p + len]) == d && len <= kMaxTieRun) ++len;
-        if (len > kMaxTieRun) {
-            too_long = true;
-            continue;
-        }
-        for (int x = 1; x < len; ++x) {
-            const uint64_t kx = keys[p + x];
-            const int32_t gx = __ldg(&slot_gi[(uint32_t)kx]);
-            int y = x - 1;
-            while (y >= 0 && __ldg(&slot_gi[(uint32_t)keys[p + y]]) > gx) {
-                keys[p + y + 1] = keys[p + y];
-                --y;
-            }
-            keys[p + y + 1] = kx;
-        }
-    }
-    return too_long;
-}
-
-template <int IPT>
-__device__ void sort_tile_smem(const TileSortArgs& a, const int64_t start, const int m, const SortSmem& sm)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    uint64_t k[IPT];
-    int32_t v[IPT];
-    uint64_t o = 0, n = ~0ull;
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const int p = warp * 32 * IPT + i * 32 + lane;
-        if (p < m) {
-            k[i] = a.keys[start + p];
-            v[i] = (int32_t)(uint32_t)k[i];
-            o |= k[i];
-            n &= k[i];
-        } else {
-            k[i] = ~0ull;  // pads rank last and are never written
-            v[i] = 0;
-        }
-    }
-    const uint64_t vary = varying_bits_block(o, n, sm.red) & 0xFFFFFFFF00000000ull;
-    if (!smem_sort<IPT>(k, v, vary, sm)) {
-        // one depth for the whole tile: keys to shared memory as they are
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) sm.k[warp * 32 * IPT + i * 32 + lane] = k[i];
-        __syncthreads();
-    }
-    const bool too_long = fix_tie_runs<IPT, 32>(sm.k, m, warp * 32 * IPT + lane, a.slot_gi);
-    if (__syncthreads_or(too_long)) {
-        // a long run of equal depths: sort again on (depth, index)
-        o = 0;
-        n = ~0ull;
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const int p = warp * 32 * IPT + i * 32 + lane;
-            if (p < m) {
-                k[i] = (k[i] & 0xFFFFFFFF00000000ull) | (uint32_t)__ldg(&a.slot_gi[v[i]]);
-                o |= k[i];
-                n &= k[i];
-            }
-        }
-        smem_sort<IPT>(k, v, varying_bits_block(o, n, sm.red), sm);
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) {
-            const int p = warp * 32 * IPT + i * 32 + lane;
-            if (p < m) a.vals[start + p] = v[i];
-        }
-        return;
-    }
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const int p = warp * 32 * IPT + i * 32 + lane;
-        if (p < m) a.vals[start + p] = (int32_t)(uint32_t)sm.k[p];
-    }
-}
+using tilesort::Smem;
 
 // One stable LSD pass of a tile too large for shared memory, by one CTA:
 // digit histogram of the segment, then 4096-key chunks in order, each
 // ranked in the block and written at its digits' running starts.
 __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t* out_k, int32_t* out_v, const int m,
-                            const int shift, const SortSmem& sm)
+                            const int shift, const Smem& sm)
 {
     constexpr int IPT = kTileSortSmemKeys / kThreads;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -450,7 +270,7 @@ __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t*
     __syncthreads();
     for (int p = threadIdx.x; p < m; p += kThreads) atomicAdd(&hist[(unsigned)(in_k[p] >> shift) & 0xFFu], 1u);
     __syncthreads();
-    const int ex = (int)excl_scan_block((int64_t)hist[threadIdx.x], sm.scan);
+    const int ex = tilesort::excl_scan<kThreads>((int)hist[threadIdx.x], sm.scan);
     sm.run[threadIdx.x] = ex;
     __syncthreads();
     for (int c0 = 0; c0 < m; c0 += kTileSortSmemKeys) {
@@ -468,7 +288,7 @@ __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t*
             }
         }
         int pos[IPT];
-        block_rank<IPT>(k, shift, pos, sm);
+        tilesort::block_rank<kThreads, IPT>(k, shift, pos, sm);
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
             const int p = c0 + warp * 32 * IPT + i * 32 + lane;
@@ -485,7 +305,7 @@ __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t*
     }
 }
 
-__device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, const int m, const SortSmem& sm)
+__device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, const int m, const Smem& sm)
 {
     uint64_t* bk[2] = {a.keys + start, a.keys_alt + start};
     int32_t* bv[2] = {a.vals + start, a.vals_alt + start};
@@ -499,7 +319,7 @@ __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, con
             o |= x;
             n &= x;
         }
-        return varying_bits_block(o, n, sm.red) & hi_mask;
+        return tilesort::varying_bits<kThreads>(o, n, sm.red) & hi_mask;
     };
     auto run_passes = [&](uint64_t mask) {
         while (mask) {
@@ -533,183 +353,25 @@ __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, con
     }
 }
 
+template <int IPT>
+__device__ void sort_big_smem(const TileSortArgs& a, const int64_t start, const int m, const Smem& sm)
+{
+    tilesort::sort_tile<kThreads, IPT>(a.keys + start, m, a.slot_gi, sm);
+    for (int p = threadIdx.x; p < m; p += kThreads) a.vals[start + p] = (int32_t)(uint32_t)sm.k[p];
+}
+
 }  // namespace
 
-// ---- warp sort: tiles of at most kWarpTile keys -----------------------------------
-//
-// One warp per tile, no block barrier: the keys sit in registers (IPT per
-// lane, item p = i * 32 + lane), each LSD pass ranks them with a per-warp
-// digit histogram (match.any peers) and scatters them through the warp's
-// shared-memory buffer.  A tile with two equal depths goes to the CTA sort,
-// which also orders ties by Gaussian index.
-
-template <int IPT>
-__device__ __forceinline__ void warp_rank(const uint64_t (&k)[IPT], const int shift, int (&pos)[IPT], uint32_t* hist)
-{
-    const int lane = threadIdx.x & 31;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) hist[lane + 32 * j] = 0;
-    __syncwarp();
-    const unsigned lt = lanemask_lt();
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const unsigned d = (unsigned)(k[i] >> shift) & 0xFFu;
-        const unsigned peers = __match_any_sync(kFull, d);
-        const uint32_t before = hist[d];
-        const int below = __popc(peers & lt);
-        __syncwarp();
-        if (below == 0) hist[d] = before + __popc(peers);
-        __syncwarp();
-        pos[i] = (int)before + below;
-    }
-    // exclusive scan of the 256 bins, 8 per lane
-    uint32_t c[8], run = 0;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-        c[j] = hist[8 * lane + j];
-        const uint32_t x = c[j];
-        c[j] = run;
-        run += x;
-    }
-    uint32_t incl = run;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t t = __shfl_up_sync(kFull, incl, o);
-        if (lane >= o) incl += t;
-    }
-    const uint32_t base = incl - run;
-    __syncwarp();
-#pragma unroll
-    for (int j = 0; j < 8; ++j) hist[8 * lane + j] = base + c[j];
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) pos[i] += (int)hist[(unsigned)(k[i] >> shift) & 0xFFu];
-    __syncwarp();
-}
-
-template <int IPT>
-__device__ void warp_sort_tile(const TileSortArgs& a, const int64_t t, const int64_t start, const int m, uint64_t* buf,
-                               uint32_t* hist)
-{
-    const int lane = threadIdx.x & 31;
-    uint64_t k[IPT];
-    uint64_t o = 0, n = ~0ull;
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const int p = i * 32 + lane;
-        if (p < m) {
-            k[i] = a.keys[start + p];
-            o |= k[i];
-            n &= k[i];
-        } else {
-            k[i] = ~0ull;
-        }
-    }
-#pragma unroll
-    for (int s = 16; s >= 1; s >>= 1) {
-        o |= __shfl_xor_sync(kFull, o, s);
-        n &= __shfl_xor_sync(kFull, n, s);
-    }
-    uint64_t mask = (o ^ n) & 0xFFFFFFFF00000000ull;
-    while (mask) {
-        const int shift = __ffsll((long long)mask) - 1;
-        mask &= ~(0xFFull << shift);
-        int pos[IPT];
-        warp_rank<IPT>(k, shift, pos, hist);
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) buf[pos[i]] = k[i];
-        __syncwarp();
-#pragma unroll
-        for (int i = 0; i < IPT; ++i) k[i] = buf[i * 32 + lane];
-        __syncwarp();
-    }
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) buf[i * 32 + lane] = k[i];
-    __syncwarp();
-    const bool too_long = fix_tie_runs<IPT, 32>(buf, m, lane, a.slot_gi);
-    if (__any_sync(kFull, too_long)) {
-        // the CTA sort re-sorts the tile on (depth, index)
-        if (lane == 0) a.mid_list[atomicAdd(a.mid_count, 1u)] = (int32_t)t;
-        return;
-    }
-    __syncwarp();
-#pragma unroll
-    for (int i = 0; i < IPT; ++i) {
-        const int p = i * 32 + lane;
-        if (p < m) a.vals[start + p] = (int32_t)(uint32_t)buf[p];
-    }
-}
-
-__global__ void __launch_bounds__(kThreads, 4) tile_sort_warp_kernel(TileSortArgs a)
-{
-    __shared__ uint64_t s_buf[kWarps][kWarpTile];
-    __shared__ uint32_t s_hist[kWarps][256];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int64_t t = (int64_t)blockIdx.x * kWarps + warp;
-    if (t >= a.tiles) return;
-    const int64_t start = __ldg(&a.ranges[2 * t]);
-    const int m = __ldg(&a.ranges[2 * t + 1]) - (int)start;
-    if (m <= 1 || m > kWarpTile) {
-        if (m == 1 && lane == 0) a.vals[start] = (int32_t)(uint32_t)a.keys[start];
-        return;
-    }
-    uint64_t* buf = s_buf[warp];
-    uint32_t* hist = s_hist[warp];
-    if (m <= 32)
-        warp_sort_tile<1>(a, t, start, m, buf, hist);
-    else if (m <= 64)
-        warp_sort_tile<2>(a, t, start, m, buf, hist);
-    else if (m <= 128)
-        warp_sort_tile<4>(a, t, start, m, buf, hist);
-    else
-        warp_sort_tile<8>(a, t, start, m, buf, hist);
-}
-
-// ---- CTA sorts over the tile lists --------------------------------------------------
-
-// Tiles of at most kMidTile keys (and warp-sort ties): persistent CTAs over
-// the mid list, high occupancy.
-__global__ void __launch_bounds__(kThreads, 4) tile_sort_mid_kernel(TileSortArgs a)
-{
-    extern __shared__ __align__(16) unsigned char smem[];
-    __shared__ int32_t s_bexcl[256];
-    __shared__ int32_t s_dcount[256];
-    __shared__ int64_t s_scan[kWarps];
-    __shared__ uint64_t s_red[2 * kWarps];
-    SortSmem sm;
-    sm.k = reinterpret_cast<uint64_t*>(smem);
-    sm.v = reinterpret_cast<int32_t*>(smem + kMidTile * 8);
-    sm.whist = reinterpret_cast<uint32_t*>(smem);
-    sm.bexcl = s_bexcl;
-    sm.dcount = s_dcount;
-    sm.scan = s_scan;
-    sm.red = s_red;
-    sm.run = nullptr;
-    const int nmid = (int)*a.mid_count;
-    for (int j = blockIdx.x; j < nmid; j += gridDim.x) {
-        const int64_t t = a.mid_list[j];
-        const int64_t start = __ldg(&a.ranges[2 * t]);
-        const int m = __ldg(&a.ranges[2 * t + 1]) - (int)start;
-        if (m <= 256)
-            sort_tile_smem<1>(a, start, m, sm);
-        else if (m <= 512)
-            sort_tile_smem<2>(a, start, m, sm);
-        else
-            sort_tile_smem<4>(a, start, m, sm);
-        __syncthreads();  // shared memory is reused by the next tile
-    }
-}
-
-// Tiles above kMidTile keys: persistent CTAs over the big list.
+// Persistent CTAs over the big-tile list.
 __global__ void __launch_bounds__(kThreads, 2) tile_sort_big_kernel(TileSortArgs a)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int32_t s_bexcl[256];
     __shared__ int32_t s_dcount[256];
     __shared__ int32_t s_run[256];
-    __shared__ int64_t s_scan[kWarps];
+    __shared__ int32_t s_scan[kWarps];
     __shared__ uint64_t s_red[2 * kWarps];
-    SortSmem sm;
+    Smem sm;
     sm.k = reinterpret_cast<uint64_t*>(smem);
     sm.v = reinterpret_cast<int32_t*>(smem + kTileSortSmemKeys * 8);
     sm.whist = reinterpret_cast<uint32_t*>(smem);
@@ -724,9 +386,9 @@ __global__ void __launch_bounds__(kThreads, 2) tile_sort_big_kernel(TileSortArgs
         const int64_t start = __ldg(&a.ranges[2 * t]);
         const int m = __ldg(&a.ranges[2 * t + 1]) - (int)start;
         if (m <= 2048)
-            sort_tile_smem<8>(a, start, m, sm);
+            sort_big_smem<8>(a, start, m, sm);
         else if (m <= kTileSortSmemKeys)
-            sort_tile_smem<16>(a, start, m, sm);
+            sort_big_smem<16>(a, start, m, sm);
         else
             sort_tile_global(a, start, m, sm);
         __syncthreads();  // shared memory is reused by the next tile
@@ -735,7 +397,6 @@ __global__ void __launch_bounds__(kThreads, 2) tile_sort_big_kernel(TileSortArgs
 
 void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st)
 {
-    constexpr int mid_smem = kMidTile * 12;
     constexpr int big_smem = kTileSortSmemKeys * 12;
     static bool attr = false;
     if (!attr) {
@@ -743,8 +404,6 @@ void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st)
         attr = true;
     }
     if (a.tiles <= 0) return;
-    tile_sort_warp_kernel<<<(unsigned)((a.tiles + kWarps - 1) / kWarps), kThreads, 0, st>>>(a);
-    tile_sort_mid_kernel<<<(unsigned)(4 * num_sms), kThreads, mid_smem, st>>>(a);
     tile_sort_big_kernel<<<(unsigned)(2 * num_sms), kThreads, big_smem, st>>>(a);
 }
 

@@ -88,10 +88,9 @@ struct TileScanArgs {
     int64_t capacity;
     int64_t* sort_n;                 // min(K, capacity)
     int* overflow;                   // K > capacity
-    int32_t* mid_list;               // out: tiles with kWarpTile < keys <= kMidTile
-    unsigned int* mid_count;
-    int32_t* big_list;               // out: tiles with more than kMidTile keys
+    int32_t* big_list;               // out: tiles with more than fused_cap keys
     unsigned int* big_count;
+    int32_t fused_cap;
 };
 
 // Per-tile sort of the buckets: each tile's keys are ordered by depth and,
@@ -105,14 +104,14 @@ struct TileSortArgs {
     int32_t* vals;                   // out: slots in blend order
     int32_t* vals_alt;
     const int32_t* slot_gi;
-    int32_t* mid_list;               // tiles for the CTA sort (from the tile scan, plus warp-sort ties)
-    unsigned int* mid_count;
-    const int32_t* big_list;         // tiles above kMidTile keys (from the tile scan)
+    const int32_t* big_list;         // tiles above the fused capacity (from the tile scan)
     const unsigned int* big_count;
 };
 constexpr int kTileSortSmemKeys = 4096;
-constexpr int kWarpTile = 256;       // tiles up to this many keys are sorted by one warp
-constexpr int kMidTile = 1024;       // ... up to this many by one high-occupancy CTA
+// Keys a tile may have to be sorted inside its raster CTA (TW * TH / 2
+// threads, 8 keys each); larger tiles are sorted ahead of the raster.
+constexpr int kFusedIpt = 8;
+inline int fused_tile_capacity(int tile_w, int tile_h) { return tile_w * tile_h / 2 * kFusedIpt; }
 constexpr int kTileScanItems = 4096;  // tiles per scan block
 
 struct EmitArgs {
@@ -171,6 +170,13 @@ struct RasterArgs {
     const float4* rec;                // 3 float4 per value (record kernel); null: use xy/conic/color
     float t_min;
     unsigned long long* tile_counter; // persistent variant only
+    // tile-bucket frames: a tile of at most fused_cap keys is sorted by its
+    // raster CTA from the bucketed (depth << 32 | slot) keys; `values` then
+    // only holds the order of the larger tiles.  keys == null: `values`
+    // holds every tile's order.
+    const uint64_t* keys;
+    const int32_t* slot_gi;
+    int32_t fused_cap;
 };
 
 void launch_sh_stage(int64_t n, const float4* pos, const float* sh, int sh_count, int deg, const ViewParams& v,

@@ -25,6 +25,7 @@
 // persistent grid that pulls global tile ids (all views' tiles, flattened)
 // from an atomic queue.
 #include "gs_kernels.h"
+#include "gs_tilesort.cuh"
 
 #include <algorithm>
 
@@ -187,6 +188,62 @@ __device__ __forceinline__ void store_pixel(const ViewParams& v, const int px, c
     v.out[(int64_t)py * v.width + px] = qc;
 }
 
+// ---- per-tile sort inside the raster CTA ----------------------------------------
+//
+// In tile-bucket frames a tile of at most fused_cap keys arrives unsorted;
+// its CTA orders it in shared memory (gs_tilesort.cuh) before blending and
+// reads the slots from there.  Larger tiles were sorted ahead of the raster
+// and are read from `values`.
+
+template <int NT>
+struct FusedSortSmem {
+    uint64_t k[NT * kFusedIpt];
+    int32_t v[NT * kFusedIpt];
+    int32_t bexcl[256];
+    int32_t dcount[256];
+    int32_t scan[NT / 32];
+    uint64_t red[2 * (NT / 32)];
+};
+
+// Returns the tile's sorted keys in shared memory, or null when the order
+// is in a.values.  Every thread of the CTA must call it.
+template <int NT>
+__device__ __forceinline__ const uint64_t* fused_sort(const RasterArgs& a, const int first, const int count,
+                                                      FusedSortSmem<NT>& fs)
+{
+    if (!a.keys || count > a.fused_cap) return nullptr;
+    if (count == 1) {
+        if (threadIdx.x == 0) fs.k[0] = a.keys[first];
+        __syncthreads();
+        return fs.k;
+    }
+    tilesort::Smem sm;
+    sm.k = fs.k;
+    sm.v = fs.v;
+    sm.whist = reinterpret_cast<uint32_t*>(fs.k);
+    sm.bexcl = fs.bexcl;
+    sm.dcount = fs.dcount;
+    sm.scan = fs.scan;
+    sm.red = fs.red;
+    sm.run = nullptr;
+    const uint64_t* src = a.keys + first;
+    if (count <= NT)
+        tilesort::sort_tile<NT, 1>(src, count, a.slot_gi, sm);
+    else if (count <= 2 * NT)
+        tilesort::sort_tile<NT, 2>(src, count, a.slot_gi, sm);
+    else if (count <= 4 * NT)
+        tilesort::sort_tile<NT, 4>(src, count, a.slot_gi, sm);
+    else
+        tilesort::sort_tile<NT, 8>(src, count, a.slot_gi, sm);
+    return fs.k;
+}
+
+// Slot of the idx-th entry of the tile whose list starts at `first`.
+__device__ __forceinline__ int slot_at(const RasterArgs& a, const uint64_t* sk, const int first, const int idx)
+{
+    return sk ? (int)(uint32_t)sk[idx] : __ldg(&a.values[first + idx]);
+}
+
 // ---- GS_TERM_REFERENCE ------------------------------------------------------------
 //
 // The reference's blend and termination, bit for bit: every pixel evaluates
@@ -205,7 +262,7 @@ struct RefSmem {
 
 template <int TW, int TH>
 __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewParams& v, const int64_t gtile,
-                                                const int local_tile, RefSmem& sm)
+                                                const int local_tile, RefSmem& sm, FusedSortSmem<TW * TH / 2>& fs)
 {
     constexpr int WX = TW / 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -226,6 +283,7 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
         }
         return;
     }
+    const uint64_t* sk = fused_sort<TW * TH / 2>(a, first, count, fs);
     // pixel corner sample, gaussian_render.cu:701-704
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy0 = (float)py0 * v.texel_y - 1.0f;
@@ -235,9 +293,9 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
     const RasterSmem rs = {sm.xy, sm.con, sm.col, nullptr};
     const bool loader = threadIdx.x < 32;
     const int t = (int)threadIdx.x;
-    if (loader && t < count) stage_entry(a, __ldg(&a.values[first + t]), rs, t);
+    if (loader && t < count) stage_entry(a, slot_at(a, sk, first, t), rs, t);
     cp_async_commit();
-    int idx_next = (loader && 32 + t < count) ? __ldg(&a.values[first + 32 + t]) : 0;
+    int idx_next = (loader && 32 + t < count) ? slot_at(a, sk, first, 32 + t) : 0;
     cp_async_wait_all();
     __syncthreads();
     for (int base = 0; base < count; base += 32) {
@@ -246,7 +304,7 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
         if (loader && base + 32 + t < count) stage_entry(a, idx_next, rs, 32 * (buf ^ 1) + t);
         cp_async_commit();
         const int n2 = base + 64 + t;
-        const int idx2 = (loader && n2 < count) ? __ldg(&a.values[first + n2]) : 0;
+        const int idx2 = (loader && n2 < count) ? slot_at(a, sk, first, n2) : 0;
         const float2* bxy = sm.xy + 32 * buf;
         const float4* bcon = sm.con + 32 * buf;
         const float4* bcol = sm.col + 32 * buf;
@@ -271,17 +329,19 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
 }
 
 template <int TW, int TH>
-__global__ void __launch_bounds__(TW * TH / 2) raster_ref_kernel(RasterArgs a)
+__global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_ref_kernel(RasterArgs a)
 {
     __shared__ RefSmem sm;
-    raster_ref_tile<TW, TH>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, sm);
+    __shared__ FusedSortSmem<TW * TH / 2> fs;
+    raster_ref_tile<TW, TH>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, sm, fs);
 }
 
 // Persistent variant over the flattened tiles of all views.
 template <int TW, int TH>
-__global__ void __launch_bounds__(TW * TH / 2) raster_ref_persistent_kernel(RasterArgs a)
+__global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_ref_persistent_kernel(RasterArgs a)
 {
     __shared__ RefSmem sm;
+    __shared__ FusedSortSmem<TW * TH / 2> fs;
     __shared__ int64_t s_tile;
     for (;;) {
         __syncthreads();
@@ -298,7 +358,7 @@ __global__ void __launch_bounds__(TW * TH / 2) raster_ref_persistent_kernel(Rast
                 hi = mid - 1;
         }
         const ViewParams& v = a.views[lo];
-        raster_ref_tile<TW, TH>(a, v, gtile, (int)(gtile - v.tile_offset), sm);
+        raster_ref_tile<TW, TH>(a, v, gtile, (int)(gtile - v.tile_offset), sm, fs);
     }
 }
 
@@ -380,13 +440,14 @@ __device__ __forceinline__ void blend_rec(const float dy, const float adx2, cons
 
 
 template <int TW, int TH>
-__global__ void __launch_bounds__(TW * TH / 2) raster_rec_kernel(RasterArgs a)
+__global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kernel(RasterArgs a)
 {
     constexpr int NW = TW * TH / 64;
     constexpr int WX = TW / 8;
     __shared__ float4 s_q0[NW][32];
     __shared__ float4 s_q1[NW][32];
     __shared__ float s_qb[NW][32];
+    __shared__ FusedSortSmem<TW * TH / 2> fs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t gtile = blockIdx.x;
     int vi = 0;
@@ -416,6 +477,7 @@ __global__ void __launch_bounds__(TW * TH / 2) raster_rec_kernel(RasterArgs a)
         }
         return;
     }
+    const uint64_t* sk = fused_sort<TW * TH / 2>(a, first, last - first, fs);
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy0 = (float)py0 * v.texel_y - 1.0f;
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
@@ -434,7 +496,7 @@ __global__ void __launch_bounds__(TW * TH / 2) raster_rec_kernel(RasterArgs a)
         float4 q0, q2;
         const float4* rp = nullptr;
         if (j < last) {
-            const int s = __ldg(&a.values[j]);
+            const int s = slot_at(a, sk, first, j - first);
             rp = a.rec + 3 * (int64_t)s;
             q0 = __ldg(rp);
             q2 = __ldg(rp + 2);
