@@ -150,6 +150,7 @@ struct gs_ctx {
     int64_t key_capacity = 0;
     int64_t per_view_capacity = 0;         // Gaussians * views the splat buffers hold
     cudaStream_t cap_stream = nullptr;     // graph capture
+    bool tile_count_dirty = true;          // tile counts may be nonzero: clear before the next frame
     std::vector<FrameGraph> graphs;
     uint64_t use_clock = 0;
 };
@@ -514,6 +515,7 @@ int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams,
     if (sizeof(uint64_t) * scan_blocks > ctx->scan_status.bytes) {
         if (ctx->scan_status.ensure(sizeof(uint64_t) * scan_blocks, true)) return fail(GS_ERR_OOM, "scan status");
     }
+    if (sizeof(uint32_t) * tiles > ctx->tile_count.bytes) ctx->tile_count_dirty = true;
     if (ctx->ranges.ensure(sizeof(int32_t) * 2 * tiles) || ctx->tile_count.ensure(sizeof(uint32_t) * tiles) ||
         ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(sizeof(int32_t) * tiles))
         return fail(GS_ERR_OOM, "tile buffers");
@@ -531,7 +533,12 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     Counters* dc = ctx->counters.as<Counters>();
     GS_CUDA(cudaMemcpyAsync(ctx->views.p, ctx->h_views, sizeof(ViewParams) * p.num_views, cudaMemcpyHostToDevice, st));
     GS_CUDA(cudaMemcpyAsync(dc, ctx->h_init, sizeof(Counters), cudaMemcpyHostToDevice, st));
-    GS_CUDA(cudaMemsetAsync(ctx->tile_count.p, 0, sizeof(uint32_t) * (size_t)p.tiles_total, st));
+    // the tile counts are all zero here: cleared when allocated, re-zeroed
+    // by every tile scan, and cleared again after a failed frame
+    if (ctx->tile_count_dirty) {
+        GS_CUDA(cudaMemsetAsync(ctx->tile_count.p, 0, ctx->tile_count.bytes, st));
+        if (!capturing) ctx->tile_count_dirty = false;
+    }
     GS_CUDA(record(ctx->ev[0], st, capturing));
 
     FrameArgs fa{};
@@ -746,7 +753,7 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         ctx->h_init->epoch_scan = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
         ctx->h_init->epoch_sort = 0;
         // the second call with the same key is captured; a redone frame is not
-        const bool use_graph = g && !g->failed && g->seen >= 2 && attempts == 1;
+        const bool use_graph = g && !g->failed && g->seen >= 2 && attempts == 1 && !ctx->tile_count_dirty;
         if (use_graph && !g->exec && !capture_frame(ctx, scene, cfg, p, *g)) g->failed = 1;
         if (use_graph && g->exec) {
             GS_CUDA(cudaGraphLaunch(g->exec, st));
@@ -756,8 +763,15 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
             if (rc) return rc;
             replayed = false;
         }
-        GS_CUDA(cudaStreamSynchronize(st));
-        if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "frame look-back timed out");
+        const cudaError_t se = cudaStreamSynchronize(st);
+        if (se != cudaSuccess) {
+            ctx->tile_count_dirty = true;
+            return cuda_fail(se, "frame");
+        }
+        if (ctx->h_counters->err) {
+            ctx->tile_count_dirty = true;
+            return fail(GS_ERR_DEVICE_TIMEOUT, "frame look-back timed out");
+        }
         const int64_t K = ctx->h_counters->total;
         if (K >= (1ll << 31)) return fail(GS_ERR_CAPACITY, "more than 2^31 tile keys");
         if (!ctx->h_counters->overflow) break;
@@ -771,7 +785,7 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         stats->sh_eval_ms = 0.0;
         stats->project_ms = ms_between(ctx->ev[0], ctx->ev[1]);
         stats->build_tile_ms = ms_between(ctx->ev[2], ctx->ev[3]);
-        stats->sort_ms = ms_between(ctx->ev[3], ctx->ev[4]);
+        stats->sort_ms = ms_between(ctx->ev[3], ctx->ev[4]);  // the tiles too big for the raster CTAs
         stats->raster_ms = ms_between(ctx->ev[4], ctx->ev[5]);
         stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
         stats->num_keys = ctx->h_counters->total;

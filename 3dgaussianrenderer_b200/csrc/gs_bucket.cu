@@ -96,9 +96,13 @@ __global__ void __launch_bounds__(kThreads) tile_scan_kernel(TileScanArgs a)
     int64_t sum = 0;
 #pragma unroll
     for (int j = 0; j < IPT; ++j) {
-        c[j] = first + j < a.tiles ? __ldg(&a.count[first + j]) : 0u;
+        c[j] = first + j < a.tiles ? a.count[first + j] : 0u;
         sum += c[j];
     }
+    // leave the counts zeroed for the next frame (saves a clear per frame)
+#pragma unroll
+    for (int j = 0; j < IPT; ++j)
+        if (first + j < a.tiles && c[j]) a.count[first + j] = 0u;
     const int64_t excl = excl_scan_block(sum, s_tmp);
     if (threadIdx.x == kThreads - 1) {
         const uint64_t agg = (uint64_t)(excl + sum);
@@ -257,21 +261,25 @@ namespace {
 
 using tilesort::Smem;
 
+constexpr int kBigThreads = kThreads;
+
 // One stable LSD pass of a tile too large for shared memory, by one CTA:
 // digit histogram of the segment, then 4096-key chunks in order, each
 // ranked in the block and written at its digits' running starts.
 __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t* out_k, int32_t* out_v, const int m,
                             const int shift, const Smem& sm)
 {
-    constexpr int IPT = kTileSortSmemKeys / kThreads;
+    constexpr int NT = kBigThreads;
+    constexpr int IPT = kTileSortSmemKeys / NT;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const bool owner = threadIdx.x < 256;
     uint32_t* hist = reinterpret_cast<uint32_t*>(sm.v);  // the value buffer is unused on this path
-    hist[threadIdx.x] = 0;
+    if (owner) hist[threadIdx.x] = 0;
     __syncthreads();
-    for (int p = threadIdx.x; p < m; p += kThreads) atomicAdd(&hist[(unsigned)(in_k[p] >> shift) & 0xFFu], 1u);
+    for (int p = threadIdx.x; p < m; p += NT) atomicAdd(&hist[(unsigned)(in_k[p] >> shift) & 0xFFu], 1u);
     __syncthreads();
-    const int ex = tilesort::excl_scan<kThreads>((int)hist[threadIdx.x], sm.scan);
-    sm.run[threadIdx.x] = ex;
+    const int ex = tilesort::excl_scan<NT>(owner ? (int)hist[threadIdx.x] : 0, sm.scan);
+    if (owner) sm.run[threadIdx.x] = ex;
     __syncthreads();
     for (int c0 = 0; c0 < m; c0 += kTileSortSmemKeys) {
         uint64_t k[IPT];
@@ -288,7 +296,7 @@ __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t*
             }
         }
         int pos[IPT];
-        tilesort::block_rank<kThreads, IPT>(k, shift, pos, sm);
+        tilesort::block_rank<NT, IPT>(k, shift, pos, sm);
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
             const int p = c0 + warp * 32 * IPT + i * 32 + lane;
@@ -300,13 +308,14 @@ __device__ void global_pass(const uint64_t* in_k, const int32_t* in_v, uint64_t*
             }
         }
         __syncthreads();
-        sm.run[threadIdx.x] += sm.dcount[threadIdx.x];
+        if (owner) sm.run[threadIdx.x] += sm.dcount[threadIdx.x];
         __syncthreads();
     }
 }
 
 __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, const int m, const Smem& sm)
 {
+    constexpr int NT = kBigThreads;
     uint64_t* bk[2] = {a.keys + start, a.keys_alt + start};
     int32_t* bv[2] = {a.vals + start, a.vals_alt + start};
     int cur = 0;
@@ -314,12 +323,12 @@ __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, con
 
     auto vary_of = [&](const uint64_t hi_mask) {
         uint64_t o = 0, n = ~0ull;
-        for (int p = threadIdx.x; p < m; p += kThreads) {
+        for (int p = threadIdx.x; p < m; p += NT) {
             const uint64_t x = bk[cur][p];
             o |= x;
             n &= x;
         }
-        return tilesort::varying_bits<kThreads>(o, n, sm.red) & hi_mask;
+        return tilesort::varying_bits<NT>(o, n, sm.red) & hi_mask;
     };
     auto run_passes = [&](uint64_t mask) {
         while (mask) {
@@ -333,9 +342,9 @@ __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, con
 
     run_passes(vary_of(0xFFFFFFFF00000000ull));
     bool t = false;
-    for (int p = threadIdx.x + 1; p < m; p += kThreads) t |= (bk[cur][p] >> 32) == (bk[cur][p - 1] >> 32);
+    for (int p = threadIdx.x + 1; p < m; p += NT) t |= (bk[cur][p] >> 32) == (bk[cur][p - 1] >> 32);
     if (__syncthreads_or(t)) {
-        for (int p = threadIdx.x; p < m; p += kThreads) {
+        for (int p = threadIdx.x; p < m; p += NT) {
             const uint64_t x = bk[cur][p];
             const int32_t s = have_v ? bv[cur][p] : (int32_t)(uint32_t)x;
             bv[cur][p] = s;
@@ -347,30 +356,31 @@ __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, con
     }
     // result into a.vals
     if (!have_v) {
-        for (int p = threadIdx.x; p < m; p += kThreads) bv[0][p] = (int32_t)(uint32_t)bk[cur][p];
+        for (int p = threadIdx.x; p < m; p += NT) bv[0][p] = (int32_t)(uint32_t)bk[cur][p];
     } else if (cur == 1) {
-        for (int p = threadIdx.x; p < m; p += kThreads) bv[0][p] = bv[1][p];
+        for (int p = threadIdx.x; p < m; p += NT) bv[0][p] = bv[1][p];
     }
 }
 
 template <int IPT>
 __device__ void sort_big_smem(const TileSortArgs& a, const int64_t start, const int m, const Smem& sm)
 {
-    tilesort::sort_tile<kThreads, IPT>(a.keys + start, m, a.slot_gi, sm);
-    for (int p = threadIdx.x; p < m; p += kThreads) a.vals[start + p] = (int32_t)(uint32_t)sm.k[p];
+    tilesort::sort_tile<kBigThreads, IPT>(a.keys + start, m, a.slot_gi, sm);
+    for (int p = threadIdx.x; p < m; p += kBigThreads) a.vals[start + p] = (int32_t)(uint32_t)sm.k[p];
 }
 
 }  // namespace
 
 // Persistent CTAs over the big-tile list.
-__global__ void __launch_bounds__(kThreads, 2) tile_sort_big_kernel(TileSortArgs a)
+__global__ void __launch_bounds__(kBigThreads, 2) tile_sort_big_kernel(TileSortArgs a)
 {
+    constexpr int NW = kBigThreads / 32;
     extern __shared__ __align__(16) unsigned char smem[];
     __shared__ int32_t s_bexcl[256];
     __shared__ int32_t s_dcount[256];
     __shared__ int32_t s_run[256];
-    __shared__ int32_t s_scan[kWarps];
-    __shared__ uint64_t s_red[2 * kWarps];
+    __shared__ int32_t s_scan[NW];
+    __shared__ uint64_t s_red[2 * NW];
     Smem sm;
     sm.k = reinterpret_cast<uint64_t*>(smem);
     sm.v = reinterpret_cast<int32_t*>(smem + kTileSortSmemKeys * 8);
@@ -404,7 +414,7 @@ void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st)
         attr = true;
     }
     if (a.tiles <= 0) return;
-    tile_sort_big_kernel<<<(unsigned)(2 * num_sms), kThreads, big_smem, st>>>(a);
+    tile_sort_big_kernel<<<(unsigned)(2 * num_sms), kBigThreads, big_smem, st>>>(a);
 }
 
 }  // namespace gs

@@ -75,7 +75,7 @@ struct BucketEmitArgs {
 // cursors; the last block writes the key total.  Ranges are clamped to
 // `capacity` (a frame whose keys do not fit is flagged, never overrun).
 struct TileScanArgs {
-    const uint32_t* count;           // [tiles]
+    uint32_t* count;                 // [tiles]; zeroed again after the scan
     int64_t tiles;
     unsigned long long* cursor;      // [tiles] out: first key of the tile
     int32_t* ranges;                 // [2 * tiles] out: first, one past last
@@ -112,7 +112,7 @@ constexpr int kTileSortSmemKeys = 4096;
 // threads, 8 keys each); larger tiles are sorted ahead of the raster.
 constexpr int kFusedIpt = 8;
 inline int fused_tile_capacity(int tile_w, int tile_h) { return tile_w * tile_h / 2 * kFusedIpt; }
-constexpr int kTileScanItems = 4096;  // tiles per scan block
+constexpr int kTileScanItems = 1024;  // tiles per scan block
 
 struct EmitArgs {
     int64_t n;

@@ -94,7 +94,8 @@ __device__ __forceinline__ void block_rank(const uint64_t (&key)[IPT], const int
                                            const Smem& sm)
 {
     constexpr int NW = NT / 32;
-    constexpr int D = 256 / NT;
+    constexpr int D = NT >= 256 ? 1 : 256 / NT;  // digits per owning thread
+    const bool owner = NT <= 256 || (int)threadIdx.x < 256;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint32_t* wh = sm.whist + warp * 256;
 #pragma unroll
@@ -115,26 +116,30 @@ __device__ __forceinline__ void block_rank(const uint64_t (&key)[IPT], const int
     __syncthreads();
     int cnt[D];
     int mine = 0;
+    if (owner) {
 #pragma unroll
-    for (int dd = 0; dd < D; ++dd) {
-        const int d = threadIdx.x * D + dd;
-        int run = 0;
+        for (int dd = 0; dd < D; ++dd) {
+            const int d = threadIdx.x * D + dd;
+            int run = 0;
 #pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            const uint32_t c = sm.whist[w * 256 + d];
-            sm.whist[w * 256 + d] = (uint32_t)run;
-            run += (int)c;
+            for (int w = 0; w < NW; ++w) {
+                const uint32_t c = sm.whist[w * 256 + d];
+                sm.whist[w * 256 + d] = (uint32_t)run;
+                run += (int)c;
+            }
+            cnt[dd] = run;
+            mine += run;
         }
-        cnt[dd] = run;
-        mine += run;
     }
     int ex = excl_scan<NT>(mine, sm.scan);
+    if (owner) {
 #pragma unroll
-    for (int dd = 0; dd < D; ++dd) {
-        const int d = threadIdx.x * D + dd;
-        sm.bexcl[d] = ex;
-        sm.dcount[d] = cnt[dd];
-        ex += cnt[dd];
+        for (int dd = 0; dd < D; ++dd) {
+            const int d = threadIdx.x * D + dd;
+            sm.bexcl[d] = ex;
+            sm.dcount[d] = cnt[dd];
+            ex += cnt[dd];
+        }
     }
     __syncthreads();
 #pragma unroll
