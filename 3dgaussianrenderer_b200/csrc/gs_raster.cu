@@ -26,6 +26,7 @@
 // from an atomic queue.
 #include "gs_kernels.h"
 #include "gs_tilesort.cuh"
+#include "gs_f32x2.cuh"
 
 #include <algorithm>
 
@@ -45,21 +46,6 @@ __device__ __forceinline__ void blend(const float cx, const float cy, const floa
     const float q = k.x * dx * dx + k.z * dy * dy + 2.0f * k.y * dx * dy;
     const float density = __expf(-0.5f * q);
     const float alpha = k.w * __saturatef(density);
-    r += col.x * T * alpha;
-    g += col.y * T * alpha;
-    b += col.z * T * alpha;
-    T *= (1.0f - alpha);
-}
-
-// Reference-mode blend with the staged conic as stored (a, b, c, 0) and
-// the opacity in the colour's w, as in gaussian_render.cu:727-737.
-__device__ __forceinline__ void blend_ref(const float cx, const float cy, const float2 c, const float4 k,
-                                          const float4 col, float& r, float& g, float& b, float& T)
-{
-    const float dx = cx - c.x, dy = cy - c.y;
-    const float q = k.x * dx * dx + k.z * dy * dy + 2.0f * k.y * dx * dy;
-    const float density = __expf(-0.5f * q);
-    const float alpha = col.w * __saturatef(density);
     r += col.x * T * alpha;
     g += col.y * T * alpha;
     b += col.z * T * alpha;
@@ -249,16 +235,61 @@ __device__ __forceinline__ int slot_at(const RasterArgs& a, const uint64_t* sk, 
 // The reference's blend and termination, bit for bit: every pixel evaluates
 // every entry, in batches of 32, and after each batch the tile stops once no
 // pixel has T > 0.02.  Each warp owns an 8x8 pixel block, two pixels per
-// thread (rows y and y + 4), so the staged entry is read from shared memory
-// once for two blends.  The batches are double-buffered: the first warp
-// starts asynchronous copies (cp.async, global -> shared, no registers held)
-// of batch k + 1 and loads the indices of batch k + 2 before the tile blends
-// batch k; the barrier that ends batch k also publishes batch k + 1.
+// thread (rows y and y + 4, same column), blended as one packed f32x2 pair:
+// the pair shares dx and every per-splat operand, so one packed instruction
+// does the work of the two scalar ones with the same rounding.  The
+// reference's expression (gaussian_render.cu:727-737) as nvcc contracts it:
+//   q     = fma((2 b) dx, dy, fma(a dx, dx, (c dy) dy))
+//   alpha = opacity * sat(__expf(-0.5 q))
+//   rgb   = fma(rgb_s T, alpha, rgb);   T = T (1 - alpha)
+// Only __expf and the saturation run per pixel.  The batches are
+// double-buffered: the first warp starts asynchronous copies (cp.async,
+// global -> shared, no registers held) of batch k + 1 and loads the indices
+// of batch k + 2 before the tile blends batch k; once its own copies have
+// landed, each of its lanes rewrites its entry with every value duplicated
+// into both halves of a pair (the operand layout of the packed blend), and
+// the barrier that ends batch k publishes batch k + 1.
 struct RefSmem {
     float2 xy[64];
     float4 con[64];
     float4 col[64];
+    ulonglong2 dp[64];  // {x, x}, {y, y}
+    ulonglong2 dq[64];  // {a, a}, {c, c}
+    ulonglong2 dr[64];  // {2 b, 2 b}, {opacity, opacity}
+    ulonglong2 ds[64];  // {red, red}, {green, green}
+    f2 dbl[64];         // {blue, blue}
 };
+
+// Rewrites staged entry `slot` as duplicated pairs.  2 b is exact (a power
+// of two scaling), so forming it here changes no rounding.
+__device__ __forceinline__ void dup_entry(RefSmem& sm, const int slot)
+{
+    const float2 c = sm.xy[slot];
+    const float4 k = sm.con[slot];
+    const float4 col = sm.col[slot];
+    sm.dp[slot] = make_ulonglong2(f2_dup(c.x), f2_dup(c.y));
+    sm.dq[slot] = make_ulonglong2(f2_dup(k.x), f2_dup(k.z));
+    sm.dr[slot] = make_ulonglong2(f2_dup(2.0f * k.y), f2_dup(col.w));
+    sm.ds[slot] = make_ulonglong2(f2_dup(col.x), f2_dup(col.y));
+    sm.dbl[slot] = f2_dup(col.z);
+}
+
+__device__ __forceinline__ void blend_ref_pair(const f2 cxx, const f2 cyy, const RefSmem& sm, const int j, f2& R,
+                                               f2& G, f2& B, f2& TT)
+{
+    const ulonglong2 P = sm.dp[j], Q = sm.dq[j], S = sm.dr[j], C = sm.ds[j];
+    const f2 dxx = f2_sub(cxx, P.x);
+    const f2 dyy = f2_sub(cyy, P.y);
+    const f2 inner = f2_fma(f2_mul(Q.x, dxx), dxx, f2_mul(f2_mul(Q.y, dyy), dyy));
+    const f2 q = f2_fma(f2_mul(S.x, dxx), dyy, inner);
+    float h0, h1;
+    f2_unpack(f2_mul(f2_dup(-0.5f), q), h0, h1);
+    const f2 alpha = f2_mul(S.y, f2_pack(__saturatef(__expf(h0)), __saturatef(__expf(h1))));
+    R = f2_fma(f2_mul(C.x, TT), alpha, R);
+    G = f2_fma(f2_mul(C.y, TT), alpha, G);
+    B = f2_fma(f2_mul(sm.dbl[j], TT), alpha, B);
+    TT = f2_mul(TT, f2_sub(f2_dup(1.0f), alpha));
+}
 
 template <int TW, int TH>
 __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewParams& v, const int64_t gtile,
@@ -288,8 +319,8 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy0 = (float)py0 * v.texel_y - 1.0f;
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
-    float r0 = 0.0f, g0 = 0.0f, b0 = 0.0f, T0 = 1.0f;
-    float r1 = 0.0f, g1 = 0.0f, b1 = 0.0f, T1 = 1.0f;
+    const f2 cxx = f2_dup(cx), cyy = f2_pack(cy0, cy1);
+    f2 R = f2_dup(0.0f), G = f2_dup(0.0f), B = f2_dup(0.0f), TT = f2_dup(1.0f);
     const RasterSmem rs = {sm.xy, sm.con, sm.col, nullptr};
     const bool loader = threadIdx.x < 32;
     const int t = (int)threadIdx.x;
@@ -297,33 +328,34 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
     cp_async_commit();
     int idx_next = (loader && 32 + t < count) ? slot_at(a, sk, first, 32 + t) : 0;
     cp_async_wait_all();
+    if (loader && t < count) dup_entry(sm, t);
     __syncthreads();
     for (int base = 0; base < count; base += 32) {
         const int buf = (base >> 5) & 1;
         const int nb = min(32, count - base);
-        if (loader && base + 32 + t < count) stage_entry(a, idx_next, rs, 32 * (buf ^ 1) + t);
+        const bool more = loader && base + 32 + t < count;
+        if (more) stage_entry(a, idx_next, rs, 32 * (buf ^ 1) + t);
         cp_async_commit();
         const int n2 = base + 64 + t;
         const int idx2 = (loader && n2 < count) ? slot_at(a, sk, first, n2) : 0;
-        const float2* bxy = sm.xy + 32 * buf;
-        const float4* bcon = sm.con + 32 * buf;
-        const float4* bcol = sm.col + 32 * buf;
+        const int j0 = 32 * buf;
         if (nb == 32) {
 #pragma unroll 4
-            for (int j = 0; j < 32; ++j) {
-                blend_ref(cx, cy0, bxy[j], bcon[j], bcol[j], r0, g0, b0, T0);
-                blend_ref(cx, cy1, bxy[j], bcon[j], bcol[j], r1, g1, b1, T1);
-            }
+            for (int j = j0; j < j0 + 32; ++j) blend_ref_pair(cxx, cyy, sm, j, R, G, B, TT);
         } else {
-            for (int j = 0; j < nb; ++j) {
-                blend_ref(cx, cy0, bxy[j], bcon[j], bcol[j], r0, g0, b0, T0);
-                blend_ref(cx, cy1, bxy[j], bcon[j], bcol[j], r1, g1, b1, T1);
-            }
+            for (int j = j0; j < j0 + nb; ++j) blend_ref_pair(cxx, cyy, sm, j, R, G, B, TT);
         }
         idx_next = idx2;
         cp_async_wait_all();
+        if (more) dup_entry(sm, 32 * (buf ^ 1) + t);
+        float T0, T1;
+        f2_unpack(TT, T0, T1);
         if (__syncthreads_count((in0 && T0 > 0.02f) || (in1 && T1 > 0.02f)) == 0) break;
     }
+    float r0, r1, g0, g1, b0, b1;
+    f2_unpack(R, r0, r1);
+    f2_unpack(G, g0, g1);
+    f2_unpack(B, b0, b1);
     if (in0) store_pixel(v, px, py0, r0, g0, b0);
     if (in1) store_pixel(v, px, py1, r1, g1, b1);
 }
@@ -413,10 +445,14 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
 // tile's warps) and tests its cull extents against the block; the
 // survivors are packed in list order into per-warp shared-memory slots
 // (rank = popcount of the ballot below the lane) and every lane blends them
-// into both its pixels.  The column offset terms of the exponent are shared
-// by the two pixels.  A warp stops when all its pixels have T < t_min.
-// Blend per pixel: p = A dx^2 + B dx dy + C dy^2, alpha = opacity * 2^p,
-// w = T alpha, colour += rgb w, T -= w.
+// into both its pixels as one packed f32x2 pair.  The column terms of the
+// exponent (A dx^2, B dx) are formed once per lane in scalar arithmetic;
+// the pair shares them.  A warp stops when all its pixels are done.
+// Blend per pixel: p = A dx^2 + B dx dy + C dy^2, alpha = sat(opacity 2^p)
+// (= opacity 2^p for the positive definite conics that make p <= 0),
+// w = T alpha, colour += rgb w, T -= w; a pixel whose T falls below t_min
+// is done: its T is set to 0, so every later w is exactly 0 and its colour
+// no longer changes.
 
 __device__ __forceinline__ float ex2_approx(const float x)
 {
@@ -425,28 +461,30 @@ __device__ __forceinline__ float ex2_approx(const float x)
     return y;
 }
 
-__device__ __forceinline__ void blend_rec(const float dy, const float adx2, const float bdx, const float4 e1,
-                                          const float eb, float& r, float& g, float& b, float& T, bool& done,
-                                          const float tmin)
+__device__ __forceinline__ float mul_sat(const float a, const float b)
 {
-    const float p = fmaf(fmaf(e1.x, dy, bdx), dy, adx2);
-    const float w = T * (e1.y * ex2_approx(p));
-    r = fmaf(e1.z, w, r);
-    g = fmaf(e1.w, w, g);
-    b = fmaf(eb, w, b);
-    T -= w;
-    done = T < tmin;
+    float y;
+    asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+    return y;
 }
 
+// One survivor, as the pair reads it: scalar terms and duplicated pairs.
+struct RecSlot {
+    float4 s;       // (x, A, B, opacity)
+    ulonglong2 yc;  // {y, y}, {C, C}
+    ulonglong2 rg;  // {red, red}, {green, green}
+    f2 bl;          // {blue, blue}
+};
 
 template <int TW, int TH>
 __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kernel(RasterArgs a)
 {
     constexpr int NW = TW * TH / 64;
     constexpr int WX = TW / 8;
-    __shared__ float4 s_q0[NW][32];
-    __shared__ float4 s_q1[NW][32];
-    __shared__ float s_qb[NW][32];
+    __shared__ float4 s_s[NW][32];
+    __shared__ ulonglong2 s_yc[NW][32];
+    __shared__ ulonglong2 s_rg[NW][32];
+    __shared__ f2 s_bl[NW][32];
     __shared__ FusedSortSmem<TW * TH / 2> fs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t gtile = blockIdx.x;
@@ -483,14 +521,16 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
     const float bx0 = (float)wx0 * v.texel_x - 1.0f, bx1 = (float)(wx0 + 7) * v.texel_x - 1.0f;
     const float by0 = (float)wy0 * v.texel_y - 1.0f, by1 = (float)(wy0 + 7) * v.texel_y - 1.0f;
-    float r0 = 0.0f, g0 = 0.0f, b0 = 0.0f, T0 = 1.0f;
-    float r1 = 0.0f, g1 = 0.0f, b1 = 0.0f, T1 = 1.0f;
-    bool d0 = !in0, d1 = !in1;
+    const f2 cyy = f2_pack(cy0, cy1);
+    // pixels outside the image start done (T = 0)
+    f2 TT = f2_pack(in0 ? 1.0f : 0.0f, in1 ? 1.0f : 0.0f);
+    f2 R = f2_dup(0.0f), G = f2_dup(0.0f), B = f2_dup(0.0f);
     const float tmin = a.t_min;
     const unsigned lt = lanemask_lt();
+    bool done = !in0 && !in1;
 
     for (int base = first; base < last; base += 32) {
-        if (__all_sync(kFull, d0 && d1)) break;
+        if (__all_sync(kFull, done)) break;
         const int j = base + lane;
         bool keep = false;
         float4 q0, q2;
@@ -505,24 +545,44 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
         const unsigned bal = __ballot_sync(kFull, keep);
         if (keep) {
             const int k = __popc(bal & lt);
-            s_q0[warp][k] = q0;
-            s_q1[warp][k] = __ldg(rp + 1);
-            s_qb[warp][k] = q2.x;
+            const float4 q1 = __ldg(rp + 1);
+            s_s[warp][k] = make_float4(q0.x, q0.z, q0.w, q1.y);
+            s_yc[warp][k] = make_ulonglong2(f2_dup(q0.y), f2_dup(q1.x));
+            s_rg[warp][k] = make_ulonglong2(f2_dup(q1.z), f2_dup(q1.w));
+            s_bl[warp][k] = f2_dup(q2.x);
         }
         __syncwarp();  // slot writes visible to the whole warp
         const int cnt = __popc(bal);
         for (int k = 0; k < cnt; ++k) {
-            const float4 e0 = s_q0[warp][k];
-            const float4 e1 = s_q1[warp][k];
-            const float eb = s_qb[warp][k];
-            const float dx = cx - e0.x;
-            const float adx2 = e0.z * dx * dx;
-            const float bdx = e0.w * dx;
-            if (!d0) blend_rec(cy0 - e0.y, adx2, bdx, e1, eb, r0, g0, b0, T0, d0, tmin);
-            if (!d1) blend_rec(cy1 - e0.y, adx2, bdx, e1, eb, r1, g1, b1, T1, d1, tmin);
+            const float4 e = s_s[warp][k];
+            const ulonglong2 yc = s_yc[warp][k];
+            const ulonglong2 rg = s_rg[warp][k];
+            const float dx = cx - e.x;
+            const f2 adx2 = f2_dup(e.y * dx * dx);
+            const f2 bdx = f2_dup(e.z * dx);
+            const f2 dyy = f2_sub(cyy, yc.x);
+            const f2 p = f2_fma(f2_fma(yc.y, dyy, bdx), dyy, adx2);
+            float p0, p1;
+            f2_unpack(p, p0, p1);
+            const f2 w = f2_mul(TT, f2_pack(mul_sat(e.w, ex2_approx(p0)), mul_sat(e.w, ex2_approx(p1))));
+            R = f2_fma(rg.x, w, R);
+            G = f2_fma(rg.y, w, G);
+            B = f2_fma(s_bl[warp][k], w, B);
+            float T0, T1;
+            f2_unpack(f2_sub(TT, w), T0, T1);
+            T0 = T0 < tmin ? 0.0f : T0;
+            T1 = T1 < tmin ? 0.0f : T1;
+            TT = f2_pack(T0, T1);
         }
         __syncwarp();  // slots are rewritten by the next chunk
+        float T0, T1;
+        f2_unpack(TT, T0, T1);
+        done = T0 == 0.0f && T1 == 0.0f;
     }
+    float r0, r1, g0, g1, b0, b1;
+    f2_unpack(R, r0, r1);
+    f2_unpack(G, g0, g1);
+    f2_unpack(B, b0, b1);
     if (in0) store_pixel(v, px, py0, r0, g0, b0);
     if (in1) store_pixel(v, px, py1, r1, g1, b1);
 }
