@@ -40,6 +40,7 @@ GS_TERM_REFERENCE = 0
 GS_TERM_TMIN = 1
 GS_ORDER_BUCKETS = 0
 GS_ORDER_ONESWEEP = 1
+GS_SCENE_KEEP_ORDER = 1
 
 
 class GsError(RuntimeError):
@@ -119,6 +120,7 @@ _sig("gs_ctx_create", _I, _I, ctypes.POINTER(_P))
 _sig("gs_ctx_destroy", _I, _P)
 _sig("gs_ctx_device_bytes", _I64, _P)
 _sig("gs_scene_create", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.POINTER(_P))
+_sig("gs_scene_create_ex", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.c_uint32, ctypes.POINTER(_P))
 _sig("gs_scene_destroy", _I, _P)
 _sig("gs_scene_size", _I64, _P)
 _sig("gs_scene_device_bytes", _I64, _P)
@@ -316,7 +318,9 @@ class Scene:
     """Device-resident scene (Renderer::UploadModel)."""
 
     def __init__(self, ctx: Context, pos4: np.ndarray, sr4: np.ndarray, sh_grouped: np.ndarray | None,
-                 sh_degree: int, color4: np.ndarray | None = None):
+                 sh_degree: int, color4: np.ndarray | None = None, keep_order: bool = False):
+        """keep_order: store the Gaussians in the caller's order
+        (GS_SCENE_KEEP_ORDER) instead of Morton order of their centres."""
         self.ctx = ctx
         pos4 = np.ascontiguousarray(pos4, np.float32)
         sr4 = np.ascontiguousarray(sr4, np.float32)
@@ -324,8 +328,9 @@ class Scene:
         col = None if color4 is None else np.ascontiguousarray(color4, np.float32)
         sh = None if sh_grouped is None else np.ascontiguousarray(sh_grouped, np.float32)
         h = _P()
-        check(lib.gs_scene_create(ctx.h, n, _ptr(pos4), _ptr(sr4), _ptr(col), _ptr(sh), sh_degree,
-                                  ctypes.byref(h)), "gs_scene_create")
+        check(lib.gs_scene_create_ex(ctx.h, n, _ptr(pos4), _ptr(sr4), _ptr(col), _ptr(sh), sh_degree,
+                                     GS_SCENE_KEEP_ORDER if keep_order else 0, ctypes.byref(h)),
+              "gs_scene_create_ex")
         self.h = h
         self.n = n
         self.sh_degree = sh_degree

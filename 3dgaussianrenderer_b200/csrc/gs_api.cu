@@ -124,6 +124,7 @@ struct gs_scene {
     int32_t sh_degree = 0;
     int32_t sh_count = 0;
     DevBuf pos, sr, color, sh;
+    DevBuf orig;  // int32 caller index of each stored Gaussian; empty: caller order
 };
 
 struct gs_ctx {
@@ -338,6 +339,7 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     fa.epoch = take_epochs(ctx->epoch_scan, 1, ctx->scan_status, st);
     fa.num_tiles = blocks;
     fa.pos = scene->pos.as<float4>();
+    fa.orig = scene->orig.as<int32_t>();
     fa.sr = scene->sr.as<float4>();
     fa.sh = scene->sh.as<float>();
     fa.sh_count = scene->sh_count;
@@ -548,6 +550,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     fa.views_per_block = p.vpb;
     fa.num_tiles = p.blocks;
     fa.pos = scene->pos.as<float4>();
+    fa.orig = scene->orig.as<int32_t>();
     fa.sr = scene->sr.as<float4>();
     fa.sh = scene->sh.as<float>();
     fa.sh_count = scene->sh_count;
@@ -566,6 +569,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     fa.err = &dc->err;
     fa.tile_count = ctx->tile_count.as<uint32_t>();
     fa.slot_counter = &dc->slots;
+    fa.aggregate = p.tiles_total <= kAggregateMaxTiles;
     if (p.n > 0) launch_frame_project(fa, p.deg, st, true);
 
     TileScanArgs ta{};
@@ -590,6 +594,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
 
     BucketEmitArgs ea{};
     ea.n = p.n;
+    ea.aggregate = p.tiles_total <= kAggregateMaxTiles;
     ea.slot_count = &dc->slots;
     ea.max_slots = p.items;
     ea.views = ctx->views.as<ViewParams>();
@@ -950,14 +955,95 @@ int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
     return t;
 }
 
-int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
-                    const float* h_color, const float* h_sh, int32_t sh_degree, gs_scene** out)
+namespace {
+
+// Uploads the caller's arrays to temporaries, sorts the Gaussians by the
+// Morton code of their centres (the onesweep sort, 4 passes over 30 bits)
+// and gathers every array into the scene's buffers in that order.
+int upload_spatial(gs_ctx* ctx, gs_scene* s, int64_t n, const float* h_position, const float* h_scale_rotation,
+                   const float* h_color, const float* h_sh)
+{
+    const size_t groups = (size_t)((n + 255) / 256);
+    const size_t sh_bytes = sizeof(float) * groups * 256 * s->sh_count;
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int64_t i = 0; i < n; ++i)
+        for (int k = 0; k < 3; ++k) {
+            const float v = h_position[4 * i + k];
+            if (std::isfinite(v)) {
+                lo[k] = std::min(lo[k], v);
+                hi[k] = std::max(hi[k], v);
+            }
+        }
+    for (int k = 0; k < 3; ++k)
+        if (!(lo[k] <= hi[k])) lo[k] = hi[k] = 0.0f;
+    const int64_t max_tiles = (n + kSortMinTile - 1) / kSortMinTile;
+    // one temporary block: source arrays, key/value ping-pong, sort scratch
+    size_t off = 0;
+    auto take = [&](size_t b) {
+        const size_t o = off;
+        off += (b + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_pos = take(16 * (size_t)n), o_sr = take(16 * (size_t)n);
+    const size_t o_col = h_color ? take(16 * (size_t)n) : 0;
+    const size_t o_sh = s->sh_count && h_sh && s->sh.p ? take(sh_bytes) : 0;
+    const size_t o_k0 = take(8 * (size_t)n), o_k1 = take(8 * (size_t)n);
+    const size_t o_v0 = take(4 * (size_t)n), o_v1 = take(4 * (size_t)n);
+    const size_t o_hist = take(sizeof(uint32_t) * kMaxPasses * kRadix);
+    const size_t o_status = take(sizeof(uint64_t) * kRadix * (size_t)max_tiles);
+    const size_t o_cnt = take(sizeof(unsigned long long) * kMaxPasses);
+    const size_t o_err = take(sizeof(int));
+    char* t = nullptr;
+    cudaError_t e = cudaMalloc(&t, off);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return cuda_fail(e, "scene reorder scratch");
+    }
+    auto P = [&](size_t o) { return (void*)(t + o); };
+    e = cudaMemcpy(P(o_pos), h_position, 16 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(P(o_sr), h_scale_rotation, 16 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && h_color) e = cudaMemcpy(P(o_col), h_color, 16 * (size_t)n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess && o_sh) e = cudaMemcpy(P(o_sh), h_sh, sh_bytes, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(P(o_status), 0, sizeof(uint64_t) * kRadix * (size_t)max_tiles);
+    if (e == cudaSuccess) e = cudaMemset(P(o_err), 0, sizeof(int));
+    int passes = 0;
+    if (e == cudaSuccess) {
+        launch_morton(n, (const float4*)P(o_pos), lo, hi, (uint64_t*)P(o_k0), (int32_t*)P(o_v0), 0);
+        SortScratch sc;
+        sc.hist = (uint32_t*)P(o_hist);
+        sc.status = (uint64_t*)P(o_status);
+        sc.counters = (unsigned long long*)P(o_cnt);
+        sc.err = (int*)P(o_err);
+        sc.max_tiles = max_tiles;
+        passes = launch_sort((uint64_t*)P(o_k0), (int32_t*)P(o_v0), (uint64_t*)P(o_k1), (int32_t*)P(o_v1), n, nullptr,
+                             30, sc, 1, ctx->num_sms, 0);
+        const int32_t* perm = (const int32_t*)P(passes % 2 ? o_v1 : o_v0);
+        launch_scene_gather(n, perm, (const float4*)P(o_pos), (const float4*)P(o_sr),
+                            h_color ? (const float4*)P(o_col) : nullptr, o_sh ? (const float*)P(o_sh) : nullptr,
+                            s->sh_count, s->pos.as<float4>(), s->sr.as<float4>(),
+                            h_color ? s->color.as<float4>() : nullptr, s->sh.as<float>(), s->orig.as<int32_t>(), 0);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    }
+    int err = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&err, P(o_err), sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(t);
+    if (e != cudaSuccess) return cuda_fail(e, "scene reorder");
+    if (err) return fail(GS_ERR_DEVICE_TIMEOUT, "scene reorder: sort look-back timed out");
+    return GS_OK;
+}
+
+}  // namespace
+
+int gs_scene_create_ex(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
+                       const float* h_color, const float* h_sh, int32_t sh_degree, uint32_t flags, gs_scene** out)
 {
     if (!ctx || !out || n < 0 || !h_position || !h_scale_rotation) return fail(GS_ERR_INVALID, "null argument");
     if (sh_degree < 0 || sh_degree > 3) return fail(GS_ERR_INVALID, "sh_degree must be 0..3");
     if (sh_degree > 0 && !h_sh) return fail(GS_ERR_INVALID, "SH scene without coefficients");
     if (sh_degree == 0 && !h_color) return fail(GS_ERR_INVALID, "degree-0 scene without colours");
     if (n >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many Gaussians");
+    if (flags & ~(uint32_t)GS_SCENE_KEEP_ORDER) return fail(GS_ERR_INVALID, "unknown scene flags");
     *out = nullptr;
     GS_CUDA(cudaSetDevice(ctx->device));
     gs_scene* s = new (std::nothrow) gs_scene();
@@ -967,14 +1053,30 @@ int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float
     s->n = n;
     s->sh_degree = sh_degree;
     s->sh_count = 3 * (sh_degree + 1) * (sh_degree + 1);
+    const bool spatial = !(flags & GS_SCENE_KEEP_ORDER) && n >= 2;
     const size_t m = (size_t)std::max<int64_t>(n, 1);
     const size_t groups = (size_t)((n + 255) / 256);
     bool ok = s->pos.ensure(16 * m) == cudaSuccess && s->sr.ensure(16 * m) == cudaSuccess;
     if (ok && h_color) ok = s->color.ensure(16 * m) == cudaSuccess;
     if (ok && sh_degree > 0) ok = s->sh.ensure(sizeof(float) * std::max<size_t>(groups, 1) * 256 * s->sh_count) == cudaSuccess;
+    if (ok && spatial) ok = s->orig.ensure(4 * m) == cudaSuccess;
     if (!ok) {
         gs_scene_destroy(s);
         return fail(GS_ERR_OOM, "scene buffers");
+    }
+    if (spatial) {
+        // padding of the last SH group stays zero, as in the caller's layout
+        if (sh_degree > 0 && cudaMemset(s->sh.p, 0, s->sh.bytes) != cudaSuccess) {
+            gs_scene_destroy(s);
+            return cuda_fail(cudaGetLastError(), "scene clear");
+        }
+        const int rc = upload_spatial(ctx, s, n, h_position, h_scale_rotation, h_color, sh_degree > 0 ? h_sh : nullptr);
+        if (rc) {
+            gs_scene_destroy(s);
+            return rc;
+        }
+        *out = s;
+        return GS_OK;
     }
     cudaError_t e = cudaMemcpy(s->pos.p, h_position, 16 * (size_t)n, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(s->sr.p, h_scale_rotation, 16 * (size_t)n, cudaMemcpyHostToDevice);
@@ -989,6 +1091,12 @@ int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float
     return GS_OK;
 }
 
+int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
+                    const float* h_color, const float* h_sh, int32_t sh_degree, gs_scene** out)
+{
+    return gs_scene_create_ex(ctx, n, h_position, h_scale_rotation, h_color, h_sh, sh_degree, 0u, out);
+}
+
 int gs_scene_destroy(gs_scene* s)
 {
     if (!s) return GS_OK;
@@ -997,6 +1105,7 @@ int gs_scene_destroy(gs_scene* s)
     s->sr.release();
     s->color.release();
     s->sh.release();
+    s->orig.release();
     delete s;
     return GS_OK;
 }
@@ -1005,7 +1114,7 @@ int64_t gs_scene_size(const gs_scene* s) { return s ? s->n : 0; }
 
 int64_t gs_scene_device_bytes(const gs_scene* s)
 {
-    return s ? (int64_t)(s->pos.bytes + s->sr.bytes + s->color.bytes + s->sh.bytes) : 0;
+    return s ? (int64_t)(s->pos.bytes + s->sr.bytes + s->color.bytes + s->sh.bytes + s->orig.bytes) : 0;
 }
 
 int gs_render(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cam, const gs_render_cfg* cfg, uint8_t* d_rgba,

@@ -157,10 +157,27 @@ __device__ __forceinline__ uint32_t depth_bits(const float depth)
     return (uint32_t)(make_key(0, depth) & 0xFFFFFFFFull);
 }
 
-__device__ __forceinline__ void put_key(const BucketEmitArgs& a, const int64_t gtile, const uint32_t depth,
-                                        const int64_t slot)
+// Called by the whole warp: each lane with `has` writes one key into tile
+// `gtile`'s bucket.  With `a.aggregate`, lanes of the same tile claim their
+// positions with one atomic (see warp_count_hits for when that pays); the
+// order inside a bucket is irrelevant, the tile sort orders it.
+__device__ __forceinline__ void put_keys(const BucketEmitArgs& a, const bool has, const int64_t gtile,
+                                         const uint32_t depth, const int64_t slot)
 {
-    const unsigned long long pos = atomicAdd(&a.cursor[gtile], 1ull);
+if (!a.aggregate) {
+        if (!has) return;
+        const unsigned long long pos = atomicAdd(&a.cursor[gtile], 1ull);
+        if ((int64_t)pos < a.capacity) a.keys[pos] = ((uint64_t)depth << 32) | (uint32_t)slot;
+        return;
+    }
+    const unsigned act = __ballot_sync(kFull, has);
+    if (!has) return;
+    const unsigned grp = __match_any_sync(act, (unsigned long long)gtile);
+    const int leader = __ffs(grp) - 1;
+    unsigned long long base = 0;
+    if ((int)(threadIdx.x & 31) == leader) base = atomicAdd(&a.cursor[gtile], (unsigned long long)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    const unsigned long long pos = base + __popc(grp & lanemask_lt());
     if ((int64_t)pos < a.capacity) a.keys[pos] = ((uint64_t)depth << 32) | (uint32_t)slot;
 }
 
@@ -178,6 +195,9 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
         int4 r = make_int4(0, 0, 0, 0);
         Ell e = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         uint32_t depth = 0;
+        uint32_t m = 0;  // hit mask still to emit (rectangles of at most 32 candidates)
+        int64_t toff = 0;
+        int tiles_x = 0;
         if (slot < nslots) {
             view = (int)((int64_t)__ldg(&a.slot_gi[slot]) / a.n);
             r = unpack_rect(__ldg(&a.rect[slot]));
@@ -185,19 +205,26 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
             depth = depth_bits(__ldg(&a.z[slot]));
             if (cand <= 32) {
                 const ViewParams& v = a.views[view];
-                uint32_t m = __ldg(&a.hitmask[slot]);
-                while (m) {
-                    const int c = __ffs(m) - 1;
-                    m &= m - 1;
-                    const int gx = r.x + c % r.z, gy = r.y + c / r.z;
-                    put_key(a, v.tile_offset + gy * v.tiles_x + gx, depth, slot);
-                }
+                m = __ldg(&a.hitmask[slot]);
+                toff = v.tile_offset;
+                tiles_x = v.tiles_x;
                 cand = 0;
             } else {
                 const float2 c = __ldg(&a.xy[slot]);
                 const float4 el = __ldg(&a.ell[slot]);
                 e = {c.x, c.y, el.x, el.y, el.z, el.w};
             }
+        }
+        // one overlap per lane and step, the warp converged
+        while (__any_sync(kFull, m != 0)) {
+            const bool has = m != 0;
+            int64_t gt = 0;
+            if (has) {
+                const int c = __ffs(m) - 1;
+                m &= m - 1;
+                gt = toff + (int64_t)(r.y + c / r.z) * tiles_x + (r.x + c % r.z);
+            }
+            put_keys(a, has, gt, depth, slot);
         }
         if (__ballot_sync(kFull, cand > 0) == 0) continue;
         // warp-cooperative walk over the large rectangles
@@ -232,12 +259,15 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
             const int oexcl = __shfl_sync(kFull, excl, o);
             const int oview = __shfl_sync(kFull, view, o);
             const uint32_t od = __shfl_sync(kFull, depth, o);
+            bool hit = false;
+            int64_t gt = 0;
             if (c < total) {
                 int tile = 0;
                 const ViewParams& v = a.views[oview];
-                if (candidate_hit(oe, orr, c - oexcl, v, tile))
-                    put_key(a, v.tile_offset + tile, od, base + (threadIdx.x & ~31) + o);
+                hit = candidate_hit(oe, orr, c - oexcl, v, tile);
+                gt = v.tile_offset + tile;
             }
+            put_keys(a, hit, gt, od, base + (threadIdx.x & ~31) + o);
         }
     }
 }

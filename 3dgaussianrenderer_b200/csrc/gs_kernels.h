@@ -25,6 +25,7 @@ struct FrameArgs {
     int32_t sh_count;
     const float4* color_in;  // degree-0 scenes: colour from the model
     const ViewParams* views;
+    const int32_t* orig;  // caller index of each stored Gaussian (null: stored in caller order)
     // outputs, per view at [view * n + i]; offsets for every Gaussian, the
     // rest only for Gaussians that overlap at least one tile
     int32_t raster_mode;  // GS_TERM_REFERENCE: color/xy/conic; GS_TERM_TMIN: rec
@@ -46,10 +47,11 @@ struct FrameArgs {
     // (view, Gaussian) pairs that overlap a tile take slots from
     // `slot_counter` in any order; every per-item output above is written
     // at the slot instead of view * n + i, `offsets[slot]` receives
-    // view * n + i, and each overlapped tile's key count is added to
+    // view * n + caller index, and each overlapped tile's key count is added to
     // tile_count[view tile offset + tile].
     uint32_t* tile_count;
     unsigned long long* slot_counter;
+    int32_t aggregate;  // group same-tile count atomics of a warp (frames with few tiles)
 };
 
 // Bucket emission: every overlap of slot s is written as
@@ -69,7 +71,12 @@ struct BucketEmitArgs {
     unsigned long long* cursor;      // [tiles]
     uint64_t* keys;
     int64_t capacity;
+    int32_t aggregate;               // group same-tile cursor atomics of a warp (frames with few tiles)
 };
+
+// Frames of at most this many tiles (all views) group the same-tile atomics
+// of a warp in the frame kernel's counts and the bucket emission.
+constexpr int64_t kAggregateMaxTiles = 32768;
 
 // Exclusive scan of the per-tile key counts into tile ranges and bucket
 // cursors; the last block writes the key total.  Ranges are clamped to
@@ -211,5 +218,14 @@ void launch_ranges(const uint64_t* keys, int64_t num_items, const int64_t* d_num
                    cudaStream_t st);
 void launch_raster(const RasterArgs& a, int tile_w, int tile_h, int termination, bool persistent, int num_sms,
                    cudaStream_t st);
+
+// Scene storage order (gs_scene.cu): 30-bit Morton codes of the centres over
+// the box [lo, hi] with values = index, then the gather of every scene array
+// through the sorted permutation (orig[j] = caller index of stored j).
+void launch_morton(int64_t n, const float4* pos, const float lo[3], const float hi[3], uint64_t* keys, int32_t* vals,
+                   cudaStream_t st);
+void launch_scene_gather(int64_t n, const int32_t* perm, const float4* pos_in, const float4* sr_in,
+                         const float4* col_in, const float* sh_in, int32_t sh_count, float4* pos, float4* sr,
+                         float4* col, float* sh, int32_t* orig, cudaStream_t st);
 
 }  // namespace gs

@@ -93,9 +93,15 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
 // Returns this lane's number of overlapping tiles; for rectangles of at
 // most 32 candidates also the hit mask (bit c = candidate c overlaps).
 // With a non-null `tile_count`, every overlap also adds one to its tile's
-// count (all lanes of the warp render the same view).
+// count (all lanes of the warp render the same view).  With `aggregate`,
+// lanes that hit the same tile in one step add their number with one atomic:
+// neighbouring Gaussians of a spatially ordered scene mostly share tiles,
+// and when a frame has few tiles, many atomics on one address serialise.
+// With many tiles the atomics spread out and the grouping costs more than
+// it saves.
 __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
-                                               uint32_t& mask, uint32_t* tile_count = nullptr)
+                                               uint32_t& mask, uint32_t* tile_count = nullptr,
+                                               const bool aggregate = false)
 {
     const int lane = threadIdx.x & 31;
     const WarpCands w = warp_scan_cands(cand);
@@ -118,12 +124,17 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
         orr.w = __shfl_sync(kFull, r.w, o);
         const int oexcl = __shfl_sync(kFull, w.excl, o);
         bool hit = false;
-        if (c < w.total) {
-            int tile;
-            hit = candidate_hit(oe, orr, c - oexcl, v, tile);
-            if (hit && tile_count) atomicAdd(&tile_count[v.tile_offset + tile], 1u);
-        }
+        int tile = 0;
+        if (c < w.total) hit = candidate_hit(oe, orr, c - oexcl, v, tile);
         const unsigned bal = __ballot_sync(kFull, hit);
+if (tile_count && hit) {
+            if (aggregate) {
+                const unsigned grp = __match_any_sync(bal, tile);
+                if (lane == __ffs(grp) - 1) atomicAdd(&tile_count[v.tile_offset + tile], (unsigned)__popc(grp));
+            } else {
+                atomicAdd(&tile_count[v.tile_offset + tile], 1u);
+            }
+        }
         const unsigned bits = bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32));
         if (bits) {
             hits += __popc(bits);
@@ -225,7 +236,9 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
         }
     }
     float4 p = make_float4(0.f, 0.f, 0.f, 0.f), sr = p, cin = p;
+    int64_t gid = i;  // the Gaussian's caller index: equal depths are ordered by it
     if (valid) {
+        if (BUCKET && a.orig) gid = __ldg(&a.orig[i]);
         p = __ldg(&a.pos[i]);
         sr = __ldg(&a.sr[i]);
         if (DEG < 0) cin = __ldg(&a.color_in[i]);
@@ -252,18 +265,13 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
         Splat s;
         float4 col = cin;
         if (valid) {
-            if (DEG >= 0) {
-                const float3 d = view_dir(v, p);
-                const float3 c = sh_color<DEG, false>(d.x, d.y, d.z, s_sh + threadIdx.x, 256);
-                col = make_float4(c.x, c.y, c.z, p.w);
-            }
             s = project_gaussian(p, sr, v);
             e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
             r = tile_rect(e, v);
             cand = rect_candidates(r);
         }
         uint32_t mask;
-        const int hits = warp_count_hits(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr);
+        const int hits = warp_count_hits(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr, a.aggregate != 0);
         int64_t o_out = o;  // where this item's outputs go
         if (BUCKET) {
             const unsigned bal = __ballot_sync(kFull, hits > 0);
@@ -272,7 +280,7 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
             if ((threadIdx.x & 31) == 0) first = atomicAdd(a.slot_counter, (unsigned long long)__popc(bal));
             first = __shfl_sync(kFull, first, 0);
             o_out = (int64_t)first + __popc(bal & lanemask_lt());
-            if (hits > 0) a.offsets[o_out] = (int32_t)o;
+            if (hits > 0) a.offsets[o_out] = (int32_t)((int64_t)view * a.n + gid);
         } else {
             const int64_t off = chain_offsets(hits, a.status + (int64_t)view * a.groups, group, a.groups, epoch,
                                               a.view_total + view, a.err);
@@ -281,6 +289,13 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
         if (valid) {
             const int64_t o = o_out;
             if (hits > 0) {
+                // the colour only matters for items that reach a tile, so the
+                // SH evaluation runs after the overlap test
+                if (DEG >= 0) {
+                    const float3 d = view_dir(v, p);
+                    const float3 c = sh_color<DEG, false>(d.x, d.y, d.z, s_sh + threadIdx.x, 256);
+                    col = make_float4(c.x, c.y, c.z, p.w);
+                }
                 a.z[o] = s.z;
                 a.rect[o] = pack_rect(r);
                 a.hitmask[o] = mask;

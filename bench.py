@@ -15,6 +15,7 @@ bounded sample of the same workload.
 from __future__ import annotations
 
 import argparse
+import datetime
 import importlib
 import json
 import os
@@ -54,18 +55,27 @@ def make_workload(gs, rank=0):
 
 
 class Clocks:
-    """nvidia-smi sampling during the timed region."""
+    """nvidia-smi sampling (100 ms period) kept to the samples taken inside
+    the timed region [mark_start(), mark_end()]."""
 
     def __init__(self, index=0):
         self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+        q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.t0 = self.t1 = None
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
-                                       "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-lms", "100"], stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(1.0)  # the sampler's own start-up
         except FileNotFoundError:
             self.p = None
+
+    def mark_start(self):
+        self.t0 = time.time()
+
+    def mark_end(self):
+        self.t1 = time.time()
 
     def stop(self):
         if self.p is None:
@@ -74,17 +84,28 @@ class Clocks:
         self.p.wait()
         self.f.flush()
         self.f.seek(0)
-        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.count(",") >= 8]
+        rows = [[x.strip() for x in r.split(",")] for r in self.f.read().strip().splitlines() if r.count(",") >= 9]
         os.unlink(self.f.name)
+
+        def stamp(r):
+            try:
+                return datetime.datetime.strptime(r[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+            except ValueError:
+                return None
+
+        if self.t0 is not None and self.t1 is not None:
+            inside = [r for r in rows if stamp(r) is not None and self.t0 - 0.05 <= stamp(r) <= self.t1 + 0.05]
+            if inside:
+                rows = inside
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        sm = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        mx = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
         reasons = set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         for r in rows:
             for k, nm in enumerate(names):
-                if "Active" in r[5 + k] and "Not" not in r[5 + k]:
+                if "Active" in r[6 + k] and "Not" not in r[6 + k]:
                     reasons.add(nm)
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": sorted(reasons), "samples": len(rows)}
@@ -177,6 +198,35 @@ def run_serving(gs, rank, rate=500.0, duration_s=3.0, budget_gb=150, max_batch=1
             "scenes_m": [n / 1e6 for n in SERVE_SCENES]}
 
 
+def run_ref1024(gs, ctx, sc, dev, stream, frames=30):
+    """The single-view path in reference-compatible mode (SH degree <= 2 as
+    the reference evaluates it, tile-wide T <= 0.02 termination) on the same
+    3M-Gaussian scene at 1024x1024, the only size the reference renders:
+    the frame the reference's own CUDA pipeline is compared with.  Median of
+    `frames` frames, CUDA events around each frame call."""
+    import torch
+    eye = gs.scenes.orbit_ring(64, RING_RADIUS, seed=1000)[0]
+    cam = gs.look_at(eye, (0, 0, 0), (0, 1, 0), 50.0, 1024, 1024, 0.1, 100.0)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    rc = gs.RenderConfig.reference()
+    out = torch.empty((1024, 1024, 4), dtype=torch.uint8, device=dev)
+    for _ in range(3):
+        gs.render(ctx, scene, cam, rc, out, stream)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(frames)]
+    st = None
+    for a, b in ev:
+        a.record(stream)
+        st = gs.render(ctx, scene, cam, rc, out, stream)
+        b.record(stream)
+    torch.cuda.synchronize()
+    ms = float(np.median([a.elapsed_time(b) for a, b in ev]))
+    scene.close()
+    return {"frame_ms": ms, "keys": st["num_keys"], "workload": "3M Gaussians SH3 (clusters), 1024x1024, "
+            "reference-compatible mode, single view"}
+
+
 def run_reference(args, rank, world):
     import torch.distributed as dist
     if rank != 0:
@@ -218,11 +268,19 @@ def run_ours(args, rank, world, local_rank):
     dev = torch.device("cuda", local_rank)
     ctx = gs.Context(local_rank)
     sc, cams = make_workload(gs, rank)
+    stream = torch.cuda.current_stream(dev)
+    if args.only_ref1024:
+        # profiling case: the reference-compatible 1024x1024 frame alone
+        r = run_ref1024(gs, ctx, sc, dev, stream, frames=args.steps)
+        if rank == 0:
+            print(json.dumps({"metric": "frame_ms", "value": r["frame_ms"], "unit": "ms", "higher_is_better": False,
+                              "config": r}), flush=True)
+        ctx.close()
+        return
     sh = gs.scenes.grouped_sh(sc["sh"])
     scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
     rc = gs.RenderConfig()
     outs = [torch.empty((c.GetHeight(), c.GetWidth(), 4), dtype=torch.uint8, device=dev) for c in cams]
-    stream = torch.cuda.current_stream(dev)
 
     def step():
         return gs.render_batch(ctx, scene, cams, rc, outs, stream)
@@ -239,6 +297,8 @@ def run_ours(args, rank, world, local_rank):
     stages = {"project_ms": 0.0, "build_tile_ms": 0.0, "sort_ms": 0.0, "raster_ms": 0.0}
     launches = 0
     keys = 0
+    if clk:
+        clk.mark_start()
     e0.record(stream)
     for _ in range(args.steps):
         st = step()
@@ -248,6 +308,8 @@ def run_ours(args, rank, world, local_rank):
         keys = st["num_keys"]
     e1.record(stream)
     torch.cuda.synchronize()
+    if clk:
+        clk.mark_end()
     ms = e0.elapsed_time(e1)
     clocks = clk.stop() if clk else None
     t = torch.tensor([ms], dtype=torch.float64, device=dev)
@@ -294,6 +356,10 @@ def run_ours(args, rank, world, local_rank):
         g1.record(stream)
         torch.cuda.synchronize()
         plain_value = plain_views / (g0.elapsed_time(g1) / 1e3)
+
+    ref1024 = None
+    if not args.no_plain:
+        ref1024 = run_ref1024(gs, ctx, sc, dev, stream)
 
     served = None
     if not args.no_serve:
@@ -342,6 +408,7 @@ def run_ours(args, rank, world, local_rank):
                 "d2h_bytes_per_step": total_bytes},
         "plain_views_per_s": plain_value,
         "batched_over_plain": (value / world / plain_value) if plain_value else None,
+        "plain_ref_mode_1024": ref1024,
         "served": served,
         "roofline": roof,
         "cpu_baseline": cpu,
@@ -354,13 +421,15 @@ def run_ours(args, rank, world, local_rank):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-plain", action="store_true", help="skip the single-view leg (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg (profiling runs)")
+    ap.add_argument("--only-ref1024", action="store_true",
+                    help="time only the reference-compatible 1024x1024 single-view frame (profiling case)")
     ap.add_argument("--views", type=int, default=VIEWS,
                     help="views per batched frame (64 = the workload; fewer only for small profiling cases)")
     args = ap.parse_args()
@@ -369,7 +438,6 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        import datetime
         import torch
         import torch.distributed as dist
         if args.impl == "ours":

@@ -120,9 +120,22 @@ GS_API int64_t gs_ctx_device_bytes(const gs_ctx* ctx);
 
 /* Uploads host arrays (reference layouts above) into a device-resident,
  * immutable scene.  h_color may be NULL when sh_degree > 0; h_sh may be NULL
- * when sh_degree == 0.  sh_count = 3 * (sh_degree + 1)^2. */
+ * when sh_degree == 0.  sh_count = 3 * (sh_degree + 1)^2.
+ *
+ * The scene is stored in Morton order of the Gaussian centres (sorted on the
+ * device during the upload); each Gaussian keeps its caller index, which
+ * orders equal depths in the tile lists of GS_ORDER_BUCKETS frames, so the
+ * images are those of the caller's order.  GS_ORDER_ONESWEEP frames order
+ * equal depths by storage order: scenes that need that ordering to break
+ * ties by caller index are created with GS_SCENE_KEEP_ORDER.  The upload
+ * needs temporary device memory of about twice the scene's size. */
 GS_API int gs_scene_create(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
                     const float* h_color, const float* h_sh, int32_t sh_degree, gs_scene** out);
+/* gs_scene_create with flags: GS_SCENE_KEEP_ORDER stores the Gaussians in the
+ * caller's order (plain copies, no temporaries). */
+#define GS_SCENE_KEEP_ORDER 1u
+GS_API int gs_scene_create_ex(gs_ctx* ctx, int64_t n, const float* h_position, const float* h_scale_rotation,
+                       const float* h_color, const float* h_sh, int32_t sh_degree, uint32_t flags, gs_scene** out);
 GS_API int gs_scene_destroy(gs_scene* scene);
 GS_API int64_t gs_scene_size(const gs_scene* scene);
 GS_API int64_t gs_scene_device_bytes(const gs_scene* scene);

@@ -66,7 +66,8 @@ def _cams(gs, name):
 def test_bucket_order_equals_onesweep(gs, ctx, name, term):
     sc = SCENES[name](gs)
     sh = gs.scenes.grouped_sh(sc["sh"])
-    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    # stored in the caller's order: onesweep frames order equal depths by storage order
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3, keep_order=True)
     cams = _cams(gs, name)
     base = gs.RenderConfig.reference() if term == 0 else gs.RenderConfig()
     total = sum(c.GetWidth() * c.GetHeight() * 4 for c in cams)
@@ -85,6 +86,48 @@ def test_bucket_order_equals_onesweep(gs, ctx, name, term):
     assert np.array_equal(out[0], out[1])
     assert np.array_equal(out[(0, "single")], out[(1, "single")])
     scene.close()
+
+
+@pytest.mark.parametrize("name", list(SCENES))
+@pytest.mark.parametrize("term", [0, 1])
+def test_spatial_storage_order_renders_caller_order_images(gs, ctx, name, term):
+    """A scene stored in Morton order (the default) renders, in bucket
+    frames, the images of the same scene stored in the caller's order, bit
+    for bit: the per-item arithmetic does not depend on where an item is
+    stored, and equal depths are ordered by the caller's index (the plane
+    scenes are all ties)."""
+    sc = SCENES[name](gs)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    cams = _cams(gs, name)
+    base = gs.RenderConfig.reference() if term == 0 else gs.RenderConfig()
+    total = sum(c.GetWidth() * c.GetHeight() * 4 for c in cams)
+    out = {}
+    for keep in (True, False):
+        scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3, keep_order=keep)
+        buf = np.zeros(total, np.uint8)
+        st = gs.render_batch_host(ctx, scene, cams, gs.RenderConfig(**{**base.__dict__, "graph": 0}), buf)
+        img, _ = gs.render_host(ctx, scene, cams[0], base)
+        out[keep] = (buf, img, st["num_keys"])
+        scene.close()
+    assert out[True][2] == out[False][2]
+    assert np.array_equal(out[True][0], out[False][0])
+    assert np.array_equal(out[True][1], out[False][1])
+
+
+def test_spatial_storage_order_degree0_and_odd_sizes(gs, ctx):
+    """Degree-0 scenes (colour array gathered) and sizes that are not a
+    multiple of the 256-Gaussian SH group."""
+    for n, deg in ((1, 3), (2, 0), (257, 2), (70_001, 0), (70_001, 1)):
+        sc = gs.scenes.uniform_scene(n, seed=40 + n, sh_degree=deg)
+        sh = gs.scenes.grouped_sh(sc["sh"]) if deg > 0 else None
+        col = sc["color4"] if deg == 0 else None
+        cam = gs.look_at((0.3, 0.2, 3.0), (0, 0, 0), (0, 1, 0), 60.0, 640, 480, 0.1, 100.0)
+        imgs = []
+        for keep in (True, False):
+            scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, deg, color4=col, keep_order=keep)
+            imgs.append(gs.render_host(ctx, scene, cam, gs.RenderConfig())[0])
+            scene.close()
+        assert np.array_equal(imgs[0], imgs[1]), (n, deg)
 
 
 def test_dense_tiles_exceed_shared_memory_sort(gs, ctx):
@@ -143,7 +186,8 @@ def test_tile_list_regrows_and_redoes_frame(gs):
     ctx = gs.Context(0)
     sc = gs.scenes.uniform_scene(50_000, seed=31, log_scale_mu=-2.0)  # big splats: K >> n
     sh = gs.scenes.grouped_sh(sc["sh"])
-    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    # caller order: the onesweep frame below orders equal depths by storage order
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3, keep_order=True)
     far = gs.look_at((0, 0, 30.0), (0, 0, 0), (0, 1, 0), 60.0, 1920, 1080, 0.1, 100.0)
     near = gs.look_at((0, 0, 2.5), (0, 0, 0), (0, 1, 0), 60.0, 1920, 1080, 0.1, 100.0)
     rc = gs.RenderConfig(graph=1)
