@@ -93,6 +93,7 @@ struct Counters {
     int64_t total;                                 // K
     int64_t sort_n;                                // min(K, key capacity)
     unsigned int big_tiles;                        // tiles sorted ahead of the raster
+    unsigned int order_heads[2];                   // raster order: heavy tiles placed, others placed
     int err;
     int overflow;                                  // K > key capacity: the frame must be redone
     uint32_t epoch_scan, epoch_sort;               // look-back epochs of this frame
@@ -141,6 +142,7 @@ struct gs_ctx {
     DevBuf sort_hist, sort_status;
     DevBuf ranges;
     DevBuf tile_count, cursor, big_list;   // tile-bucket ordering: keys per tile, bucket fill cursors, big tiles
+    DevBuf tile_order;                     // raster order of the tiles (heavy tiles first)
     DevBuf counters;
     DevBuf image;                          // images of the host-output variants
     Counters* h_counters = nullptr;        // pinned mirror
@@ -519,7 +521,8 @@ int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams,
     }
     if (sizeof(uint32_t) * tiles > ctx->tile_count.bytes) ctx->tile_count_dirty = true;
     if (ctx->ranges.ensure(sizeof(int32_t) * 2 * tiles) || ctx->tile_count.ensure(sizeof(uint32_t) * tiles) ||
-        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(sizeof(int32_t) * tiles))
+        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(sizeof(int32_t) * tiles) ||
+        ctx->tile_order.ensure(sizeof(int32_t) * tiles))
         return fail(GS_ERR_OOM, "tile buffers");
     return GS_OK;
 }
@@ -589,6 +592,8 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ta.big_count = &dc->big_tiles;
     ta.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     launch_tile_scan(ta, st);
+    launch_tile_order(ctx->ranges.as<int32_t>(), p.tiles_total, &dc->total, ctx->tile_order.as<int32_t>(),
+                      dc->order_heads, st);
     GS_CUDA(record(ctx->ev[1], st, capturing));
     GS_CUDA(record(ctx->ev[2], st, capturing));
 
@@ -640,6 +645,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ra.keys = ctx->keys0.as<uint64_t>();  // tiles up to the fused capacity are sorted by the raster CTA
     ra.slot_gi = ctx->offsets.as<int32_t>();
     ra.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
+    ra.order = ctx->tile_order.as<int32_t>();
     launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, p.num_views > 1, ctx->num_sms, st);
     GS_CUDA(cudaGetLastError());
     GS_CUDA(record(ctx->ev[5], st, capturing));
@@ -652,7 +658,8 @@ uint64_t layout_of(const gs_ctx* ctx)
 {
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                             &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->keys0, &ctx->vals0,
-                            &ctx->keys1, &ctx->vals1, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->counters};
+                            &ctx->keys1, &ctx->vals1, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list,
+                            &ctx->tile_order, &ctx->counters};
     uint64_t h = 1469598103934665603ull;
     auto mix = [&h](uint64_t x) { h = (h ^ x) * 1099511628211ull; };
     for (const DevBuf* b : bufs) {
@@ -933,7 +940,8 @@ int gs_ctx_destroy(gs_ctx* ctx)
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
     DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                       &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
-                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->counters, &ctx->image};
+                      &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->tile_order,
+                      &ctx->counters, &ctx->image};
     for (DevBuf* b : bufs) b->release();
     if (ctx->h_counters) cudaFreeHost(ctx->h_counters);
     if (ctx->h_init) cudaFreeHost(ctx->h_init);
@@ -949,7 +957,8 @@ int64_t gs_ctx_device_bytes(const gs_ctx* ctx)
     if (!ctx) return 0;
     const DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                             &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
-                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->counters, &ctx->image};
+                            &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->tile_order,
+                      &ctx->counters, &ctx->image};
     int64_t t = 0;
     for (const DevBuf* b : bufs) t += (int64_t)b->bytes;
     return t;

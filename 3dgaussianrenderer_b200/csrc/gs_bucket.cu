@@ -150,6 +150,44 @@ void launch_tile_scan(const TileScanArgs& a, cudaStream_t st)
     tile_scan_kernel<<<(unsigned)blocks, kThreads, 0, st>>>(a);
 }
 
+// ---- 1b. raster order of the tiles --------------------------------------------
+//
+// Tiles with more than 1.5x the average key count go first, so the longest
+// raster CTAs start in the first wave instead of stretching the last one;
+// the others follow (in reverse order, filled from the end).  One atomic
+// per warp and class.
+__global__ void __launch_bounds__(kThreads) tile_order_kernel(const int32_t* __restrict__ ranges, int64_t tiles,
+                                                             const int64_t* __restrict__ total,
+                                                             int32_t* __restrict__ order, unsigned int* heads)
+{
+    const int64_t t = (int64_t)blockIdx.x * kThreads + threadIdx.x;
+    const bool valid = t < tiles;
+    const int64_t cnt = valid ? (int64_t)(__ldg(&ranges[2 * t + 1]) - __ldg(&ranges[2 * t])) : 0;
+    const bool heavy = valid && 2 * cnt * tiles > 3 * *total;
+    const unsigned bh = __ballot_sync(kFull, heavy), bl = __ballot_sync(kFull, valid && !heavy);
+    const int lane = threadIdx.x & 31;
+    unsigned int h0 = 0, l0 = 0;
+    if (lane == 0) {
+        if (bh) h0 = atomicAdd(&heads[0], (unsigned)__popc(bh));
+        if (bl) l0 = atomicAdd(&heads[1], (unsigned)__popc(bl));
+    }
+    h0 = __shfl_sync(kFull, h0, 0);
+    l0 = __shfl_sync(kFull, l0, 0);
+    const unsigned below = lanemask_lt();
+    if (heavy)
+        order[h0 + __popc(bh & below)] = (int32_t)t;
+    else if (valid)
+        order[tiles - 1 - (int64_t)(l0 + __popc(bl & below))] = (int32_t)t;
+}
+
+void launch_tile_order(const int32_t* ranges, int64_t tiles, const int64_t* total, int32_t* order,
+                       unsigned int* heads, cudaStream_t st)
+{
+    if (tiles <= 0) return;
+    tile_order_kernel<<<(unsigned)((tiles + kThreads - 1) / kThreads), kThreads, 0, st>>>(ranges, tiles, total, order,
+                                                                                         heads);
+}
+
 // ---- 2. bucket emit -----------------------------------------------------------
 
 __device__ __forceinline__ uint32_t depth_bits(const float depth)

@@ -184,6 +184,7 @@ struct RasterArgs {
     const uint64_t* keys;
     const int32_t* slot_gi;
     int32_t fused_cap;
+    const int32_t* order;             // non-null: CTA (or queue entry) k rasterises tile order[k]
 };
 
 void launch_sh_stage(int64_t n, const float4* pos, const float* sh, int sh_count, int deg, const ViewParams& v,
@@ -192,6 +193,10 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
                           float* z, float4* ell, float4* conic, cudaStream_t st);
 void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st, bool bucket = false);
 void launch_tile_scan(const TileScanArgs& a, cudaStream_t st);
+// Raster order of the tiles: those with more than 1.5x the average key count
+// (ranges and *total from the tile scan) first.  heads[2] start at zero.
+void launch_tile_order(const int32_t* ranges, int64_t tiles, const int64_t* total, int32_t* order,
+                       unsigned int* heads, cudaStream_t st);
 void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st);
 void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st);
 void launch_count_stage(const FrameArgs& a, cudaStream_t st);

@@ -274,14 +274,20 @@ __device__ __forceinline__ void dup_entry(RefSmem& sm, const int slot)
     sm.dbl[slot] = f2_dup(col.z);
 }
 
-__device__ __forceinline__ void blend_ref_pair(const f2 cxx, const f2 cyy, const RefSmem& sm, const int j, f2& R,
+__device__ __forceinline__ void blend_ref_pair(const float cx, const f2 cyy, const RefSmem& sm, const int j, f2& R,
                                                f2& G, f2& B, f2& TT)
 {
     const ulonglong2 P = sm.dp[j], Q = sm.dq[j], S = sm.dr[j], C = sm.ds[j];
-    const f2 dxx = f2_sub(cxx, P.x);
+    // the column terms are the same for both pixels: one scalar operation each
+    float sx, a, b2, unused;
+    f2_unpack(P.x, sx, unused);
+    f2_unpack(Q.x, a, unused);
+    f2_unpack(S.x, b2, unused);
+    const float dx = cx - sx;
+    const f2 dxx = f2_dup(dx);
     const f2 dyy = f2_sub(cyy, P.y);
-    const f2 inner = f2_fma(f2_mul(Q.x, dxx), dxx, f2_mul(f2_mul(Q.y, dyy), dyy));
-    const f2 q = f2_fma(f2_mul(S.x, dxx), dyy, inner);
+    const f2 inner = f2_fma(f2_dup(a * dx), dxx, f2_mul(f2_mul(Q.y, dyy), dyy));
+    const f2 q = f2_fma(f2_dup(b2 * dx), dyy, inner);
     float h0, h1;
     f2_unpack(f2_mul(f2_dup(-0.5f), q), h0, h1);
     const f2 alpha = f2_mul(S.y, f2_pack(__saturatef(__expf(h0)), __saturatef(__expf(h1))));
@@ -319,7 +325,7 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy0 = (float)py0 * v.texel_y - 1.0f;
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
-    const f2 cxx = f2_dup(cx), cyy = f2_pack(cy0, cy1);
+    const f2 cyy = f2_pack(cy0, cy1);
     f2 R = f2_dup(0.0f), G = f2_dup(0.0f), B = f2_dup(0.0f), TT = f2_dup(1.0f);
     const RasterSmem rs = {sm.xy, sm.con, sm.col, nullptr};
     const bool loader = threadIdx.x < 32;
@@ -341,9 +347,9 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
         const int j0 = 32 * buf;
         if (nb == 32) {
 #pragma unroll 4
-            for (int j = j0; j < j0 + 32; ++j) blend_ref_pair(cxx, cyy, sm, j, R, G, B, TT);
+            for (int j = j0; j < j0 + 32; ++j) blend_ref_pair(cx, cyy, sm, j, R, G, B, TT);
         } else {
-            for (int j = j0; j < j0 + nb; ++j) blend_ref_pair(cxx, cyy, sm, j, R, G, B, TT);
+            for (int j = j0; j < j0 + nb; ++j) blend_ref_pair(cx, cyy, sm, j, R, G, B, TT);
         }
         idx_next = idx2;
         cp_async_wait_all();
@@ -365,7 +371,8 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_ref_kern
 {
     __shared__ RefSmem sm;
     __shared__ FusedSortSmem<TW * TH / 2> fs;
-    raster_ref_tile<TW, TH>(a, a.view0, (int64_t)blockIdx.x + a.view0.tile_offset, (int)blockIdx.x, sm, fs);
+    const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : (int64_t)blockIdx.x + a.view0.tile_offset;
+    raster_ref_tile<TW, TH>(a, a.view0, gtile, (int)(gtile - a.view0.tile_offset), sm, fs);
 }
 
 // Persistent variant over the flattened tiles of all views.
@@ -377,7 +384,10 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_ref_pers
     __shared__ int64_t s_tile;
     for (;;) {
         __syncthreads();
-        if (threadIdx.x == 0) s_tile = (int64_t)atomicAdd(a.tile_counter, 1ull);
+        if (threadIdx.x == 0) {
+            const int64_t k = (int64_t)atomicAdd(a.tile_counter, 1ull);
+            s_tile = k < a.num_tiles_total && a.order ? (int64_t)a.order[k] : k;
+        }
         __syncthreads();
         const int64_t gtile = s_tile;
         if (gtile >= a.num_tiles_total) return;
@@ -487,7 +497,7 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
     __shared__ f2 s_bl[NW][32];
     __shared__ FusedSortSmem<TW * TH / 2> fs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t gtile = blockIdx.x;
+    const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : (int64_t)blockIdx.x;
     int vi = 0;
     if (a.num_views > 1) {
         int hi = a.num_views - 1;
