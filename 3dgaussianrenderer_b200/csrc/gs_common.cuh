@@ -80,10 +80,59 @@ struct Splat {
     float ca, cb, cc;   // conic
 };
 
+// View position and clip-space centre of one Gaussian (the first half of
+// the projection, gaussian_render.cu:160-182): enough to decide the
+// frustum test, so Gaussians outside the view can skip the rest.
+struct ViewPos {
+    float vx, vy, vz;                  // view space
+    float zRcp, zRcpSqr, ftx, fty;
+    float scaleX, scaleY, shearX, shearY;
+    float cx, cy, cz;                  // clip space, before the cull
+};
+
+__device__ __forceinline__ ViewPos view_position(const float4 p, const ViewParams& v)
+{
+    ViewPos w;
+    // view * vec4(position, 1): (m0*x + m1*y) + (m2*z + m3*1)
+    // (glm/detail/type_mat4x4.inl:536-570)
+    const float* V = v.view;
+    w.vx = (V[0] * p.x + V[4] * p.y) + (V[8] * p.z + V[12] * 1.0f);
+    w.vy = (V[1] * p.x + V[5] * p.y) + (V[9] * p.z + V[13] * 1.0f);
+    w.vz = (V[2] * p.x + V[6] * p.y) + (V[10] * p.z + V[14] * 1.0f);
+
+    w.zRcp = 1.0f / w.vz;
+    w.zRcpSqr = w.zRcp * w.zRcp;
+    w.scaleX = -v.cot[0] * w.zRcp;
+    w.scaleY = -v.cot[1] * w.zRcp;
+    w.ftx = v.cot[0] * w.vx;
+    w.fty = v.cot[1] * w.vy;
+    w.shearX = w.ftx * w.zRcpSqr;
+    w.shearY = w.fty * w.zRcpSqr;
+    const float translationX = -w.ftx * w.zRcp;
+    const float translationY = -w.fty * w.zRcp;
+    // affine * vec4(viewPosition, 1) (:182)
+    w.cx = (w.scaleX * w.vx + 0.0f * w.vy) + (w.shearX * w.vz + translationX * 1.0f);
+    w.cy = (0.0f * w.vx + w.scaleY * w.vy) + (w.shearY * w.vz + translationY * 1.0f);
+    w.cz = (0.0f * w.vx + 0.0f * w.vy) + (v.dsb[0] * w.vz + v.dsb[1] * 1.0f);
+    return w;
+}
+
+// The frustum part of the reference's visibility, step(-1, clip) *
+// step(clip, 1) (:205-206): false only for a centre outside [-1, 1]^3 (a
+// NaN coordinate passes, as it does there).  The eigenvalue factor
+// step(0, lambda1) is always 1 (lambda1 = max(0, ...)), so a Gaussian
+// that fails this test is culled and overlaps no tile.
+__device__ __forceinline__ bool in_frustum(const ViewPos& w)
+{
+    return !(w.cx < -1.0f) && !(1.0f < w.cx) && !(w.cy < -1.0f) && !(1.0f < w.cy) && !(w.cz < -1.0f) &&
+           !(1.0f < w.cz);
+}
+
 // EWA projection of one Gaussian: quaternion decode, covariance
 // R S S^T R^T, affine Jacobian of the perspective divide, clip-space 2x2
 // covariance plus trace bump, eigen-decomposition, conic and frustum test.
-__device__ __forceinline__ Splat project_gaussian(const float4 p, const float4 sr, const ViewParams& v)
+// `w` is view_position(p, v).
+__device__ __forceinline__ Splat project_gaussian(const ViewPos& w, const float4 sr, const ViewParams& v)
 {
     const uint32_t bits = __float_as_uint(sr.w);
     // decodeVec4 (gaussian_render.cu:45-48), then *2 - 1 (:150)
@@ -119,23 +168,8 @@ __device__ __forceinline__ Splat project_gaussian(const float4 p, const float4 s
     const M3 RS = mul(R, S);
     const M3 cov = mul(RS, transpose(RS));
 
-    // view * vec4(position, 1): (m0*x + m1*y) + (m2*z + m3*1)
-    // (glm/detail/type_mat4x4.inl:536-570)
     const float* V = v.view;
-    const float vx = (V[0] * p.x + V[4] * p.y) + (V[8] * p.z + V[12] * 1.0f);
-    const float vy = (V[1] * p.x + V[5] * p.y) + (V[9] * p.z + V[13] * 1.0f);
-    const float vz = (V[2] * p.x + V[6] * p.y) + (V[10] * p.z + V[14] * 1.0f);
-
-    const float zRcp = 1.0f / vz;
-    const float zRcpSqr = zRcp * zRcp;
-    const float scaleX = -v.cot[0] * zRcp;
-    const float scaleY = -v.cot[1] * zRcp;
-    const float ftx = v.cot[0] * vx;
-    const float fty = v.cot[1] * vy;
-    const float shearX = ftx * zRcpSqr;
-    const float shearY = fty * zRcpSqr;
-    const float translationX = -ftx * zRcp;
-    const float translationY = -fty * zRcp;
+    const float scaleX = w.scaleX, scaleY = w.scaleY, shearX = w.shearX, shearY = w.shearY;
 
     // mat3(affine) * mat3(view) (:180), affine columns
     // (scaleX,0,0) (0,scaleY,0) (shearX,shearY,dsb.x)
@@ -151,10 +185,7 @@ __device__ __forceinline__ Splat project_gaussian(const float4 p, const float4 s
     const M3 VP = mul(A, B);
     const M3 cc = mul(mul(VP, transpose(cov)), transpose(VP));
 
-    // affine * vec4(viewPosition, 1) (:182)
-    float cx = (scaleX * vx + 0.0f * vy) + (shearX * vz + translationX * 1.0f);
-    float cy = (0.0f * vx + scaleY * vy) + (shearY * vz + translationY * 1.0f);
-    float cz = (0.0f * vx + 0.0f * vy) + (v.dsb[0] * vz + v.dsb[1] * 1.0f);
+    float cx = w.cx, cy = w.cy, cz = w.cz;
 
     const float c00 = cc.m[0][0] + v.bump_x;
     const float c11 = cc.m[1][1] + v.bump_y;
@@ -203,6 +234,11 @@ __device__ __forceinline__ Splat project_gaussian(const float4 p, const float4 s
     s.cb = -c10 * invDet;
     s.cc = c00 * invDet;
     return s;
+}
+
+__device__ __forceinline__ Splat project_gaussian(const float4 p, const float4 sr, const ViewParams& v)
+{
+    return project_gaussian(view_position(p, v), sr, v);
 }
 
 // ---- SH colour (gaussian_render.cu:50-94; degree 3: cuda_renderer.cu:119-156)

@@ -265,10 +265,15 @@ __global__ void __launch_bounds__(256, 3) frame_project_kernel(FrameArgs a)
         Splat s;
         float4 col = cin;
         if (valid) {
-            s = project_gaussian(p, sr, v);
-            e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
-            r = tile_rect(e, v);
-            cand = rect_candidates(r);
+            // outside the frustum: culled, no tile (whole warps of a
+            // spatially ordered scene skip the projection together)
+            const ViewPos w = view_position(p, v);
+            if (in_frustum(w)) {
+                s = project_gaussian(w, sr, v);
+                e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
+                r = tile_rect(e, v);
+                cand = rect_candidates(r);
+            }
         }
         uint32_t mask;
         const int hits = warp_count_hits(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr, a.aggregate != 0);
