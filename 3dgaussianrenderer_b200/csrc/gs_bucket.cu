@@ -253,16 +253,41 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
                 e = {c.x, c.y, el.x, el.y, el.z, el.w};
             }
         }
-        // one overlap per lane and step, the warp converged
-        while (__any_sync(kFull, m != 0)) {
-            const bool has = m != 0;
-            int64_t gt = 0;
-            if (has) {
-                const int c = __ffs(m) - 1;
-                m &= m - 1;
-                gt = toff + (int64_t)(r.y + c / r.z) * tiles_x + (r.x + c % r.z);
+        if (a.aggregate) {
+            // one overlap per lane and step, the warp converged
+            while (__any_sync(kFull, m != 0)) {
+                const bool has = m != 0;
+                int64_t gt = 0;
+                if (has) {
+                    const int c = __ffs(m) - 1;
+                    m &= m - 1;
+                    gt = toff + (int64_t)(r.y + c / r.z) * tiles_x + (r.x + c % r.z);
+                }
+                put_keys(a, has, gt, depth, slot);
             }
-            put_keys(a, has, gt, depth, slot);
+        } else {
+            // up to 4 overlaps per step: their cursor atomics are in flight
+            // together, then the keys are written
+            const uint64_t lo = (uint32_t)slot;
+            while (m) {
+                int64_t gt[4];
+                unsigned long long pos[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    gt[u] = -1;
+                    if (m) {
+                        const int c = __ffs(m) - 1;
+                        m &= m - 1;
+                        gt[u] = toff + (int64_t)(r.y + c / r.z) * tiles_x + (r.x + c % r.z);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (gt[u] >= 0) pos[u] = atomicAdd(&a.cursor[gt[u]], 1ull);
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (gt[u] >= 0 && (int64_t)pos[u] < a.capacity) a.keys[pos[u]] = ((uint64_t)depth << 32) | lo;
+            }
         }
         if (__ballot_sync(kFull, cand > 0) == 0) continue;
         // warp-cooperative walk over the large rectangles
