@@ -123,9 +123,17 @@ def cpu_baseline(gs, sc, cams, sample_views=1, threads=None):
     for v in range(sample_views):
         O.render(sc, sh, cams[v], rc)
     dt = time.perf_counter() - t0
+    # work of view 0 for the raster roofline (outside the timed sample):
+    # evaluations of every splat until T < t_min, and those the GPU's
+    # warp-culled raster executes
+    O.count_block_evals(True)
+    _, _, evals, _ = O.render(sc, sh, cams[0], rc)
+    block_evals = O.block_evals()
+    O.count_block_evals(False)
     return {"value": sample_views / dt, "unit": "views/s", "cores": O.max_threads(), "kind": "port",
             "sample": f"{sample_views} of the 64 views ({cams[0].GetWidth()}x{cams[0].GetHeight()}), full frame "
-                      f"(SH3 + project + build + sort + raster) of the 3M scene, {dt:.1f} s"}
+                      f"(SH3 + project + build + sort + raster) of the 3M scene, {dt:.1f} s",
+            "evals_view0": evals, "block_evals_view0": block_evals}
 
 
 SERVE_SCENES = [200_000, 500_000, 1_000_000, 1_000_000, 2_000_000, 2_000_000, 3_000_000, 4_000_000]
@@ -343,6 +351,7 @@ def run_ours(args, rank, world, local_rank):
 
     # plain single-view path over the same views (for the batched/plain ratio)
     plain_value = None
+    raster_view0_ms = None
     if not args.no_plain:
         plain_views = min(VIEWS, 16)
         for v in range(2):
@@ -356,6 +365,11 @@ def run_ours(args, rank, world, local_rank):
         g1.record(stream)
         torch.cuda.synchronize()
         plain_value = plain_views / (g0.elapsed_time(g1) / 1e3)
+        # raster stage of view 0 alone (the raster roofline below)
+        r0 = []
+        for _ in range(10):
+            r0.append(gs.render(ctx, scene, cams[0], rc, outs[0], stream)["raster_ms"])
+        raster_view0_ms = float(np.median(r0))
 
     ref1024 = None
     if not args.no_plain:
@@ -397,6 +411,24 @@ def run_ours(args, rank, world, local_rank):
             "stage_ms": per, "stage_gbs": ach, "dominant_stage": dom,
             "dominant_bound": "fp32 + MUFU (raster blends; sort of small tiles fused in)"}
     cpu = cpu_baseline(gs, sc, cams, sample_views=1) if (world == 1 and not args.no_cpu) else None
+    # Raster roofline (FP32 pipe) of view 0 rendered alone: work = 11 FP32
+    # lane operations per (pixel, entry) evaluation of the record raster (the
+    # packed blend: exponent 2 fma + column terms, w, 3 colour fma, T update,
+    # saturation), the evaluations the GPU's warp-culled raster executes as
+    # counted by the oracle; time = the raster stage; peak = 148 SMs x 128
+    # FP32 lanes x the SM clock sampled during the timed region.  The oracle's
+    # count without culling (every entry until T < t_min) is given beside it.
+    raster_roof = None
+    if cpu and cpu.get("block_evals_view0") and raster_view0_ms:
+        clk_mhz = (clocks or {}).get("sm_mhz") or 1965.0
+        peak_gops = 148 * 128 * clk_mhz * 1e6 / 1e9
+        ach = 11.0 * cpu["block_evals_view0"] / (raster_view0_ms / 1e3) / 1e9
+        raster_roof = {"bound": "fp32", "kernel": "raster_rec (T_min records, per-tile sort fused)",
+                       "achieved": ach, "peak": peak_gops, "unit": "Gop/s", "frac": ach / peak_gops,
+                       "evals_executed": cpu["block_evals_view0"], "evals_unculled": cpu["evals_view0"],
+                       "ops_per_eval": 11, "raster_ms": raster_view0_ms,
+                       "view": f"view 0 ({cams[0].GetWidth()}x{cams[0].GetHeight()}) rendered alone",
+                       "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x sampled SM clock"}
     line = {
         "metric": "views/s", "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -411,6 +443,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_ref_mode_1024": ref1024,
         "served": served,
         "roofline": roof,
+        "raster_roofline": raster_roof,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,

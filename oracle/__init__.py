@@ -88,6 +88,8 @@ class Oracle:
             "gso_ranges": (None, [_I64, _P, _I32, _P]),
             "gso_raster": (None, [pc, pg, _P, _P, _P, _P, _P, _P, _P]),
             "gso_render": (_I64, [_I64, _P, _P, _P, _P, _I32, _I32, pc, pg, _P, _I64, _P, _P]),
+            "gso_set_count_block_evals": (None, [_I32]),
+            "gso_block_evals": (_I64, []),
         }
         for name, (res, args) in sig.items():
             fn = getattr(L, name)
@@ -105,6 +107,14 @@ class Oracle:
 
     def set_threads(self, n: int):
         self.lib.gso_set_threads(n)
+
+    def count_block_evals(self, on: bool):
+        """Counts, in later T_min rasters, the (pixel, entry) evaluations the
+        GPU's warp-culled raster executes (read with block_evals())."""
+        self.lib.gso_set_count_block_evals(1 if on else 0)
+
+    def block_evals(self) -> int:
+        return int(self.lib.gso_block_evals())
 
     def max_threads(self) -> int:
         return self.lib.gso_max_threads()

@@ -671,6 +671,79 @@ void gso_ranges(int64_t k, const uint64_t* keys, int32_t num_tiles, int32_t* ran
 
 /* ---- raster (core/gaussian_render.cu:679-759) ----------------------------- */
 
+/* Work count of the GPU's T_min raster, which has no counterpart in the
+ * reference: each warp there owns an 8x8 pixel block, walks the tile's list
+ * 32 entries at a time, keeps the entries whose cutoff box (where
+ * opacity * density = 2^-18) touches the block, blends every kept entry into
+ * all 64 pixels, and stops after a chunk once every pixel of the block has
+ * T < t_min.  gso_raster adds the (pixel, entry) evaluations that this walk
+ * executes to a counter when counting is on (the raster roofline's work);
+ * the image and the `evals` output of gso_raster are unchanged. */
+static int g_count_blocks = 0;
+static int64_t g_block_evals = 0;
+void gso_set_count_block_evals(int on)
+{
+    g_count_blocks = on;
+    g_block_evals = 0;
+}
+int64_t gso_block_evals(void) { return g_block_evals; }
+
+static const float kGsoCullAlpha = 3.814697265625e-06f; /* 2^-18 */
+
+static int64_t block_walk_evals(int tile_px0, int tile_py0, int tw, int th, int W, int H, float texx, float texy,
+                                const int32_t* list, int count, const float* xy, const float* conic4,
+                                const float* color4, float t_min)
+{
+    int64_t e = 0;
+    for (int by = 0; by < th; by += 8)
+        for (int bx = 0; bx < tw; bx += 8) {
+            const int wx0 = tile_px0 + bx, wy0 = tile_py0 + by;
+            const float bx0 = (float)wx0 * texx - 1.0f, bx1 = (float)(wx0 + 7) * texx - 1.0f;
+            const float by0 = (float)wy0 * texy - 1.0f, by1 = (float)(wy0 + 7) * texy - 1.0f;
+            float T[64];
+            int live = 0;
+            for (int p = 0; p < 64; ++p) {
+                const int px = wx0 + (p & 7), py = wy0 + (p >> 3);
+                T[p] = (px < W && py < H) ? 1.0f : 0.0f;
+                live += T[p] > 0.0f;
+            }
+            for (int c0 = 0; c0 < count && live; c0 += 32) {
+                const int nb = count - c0 < 32 ? count - c0 : 32;
+                for (int j = 0; j < nb; ++j) {
+                    const int32_t s = list[c0 + j];
+                    const float x = xy[2 * s], y = xy[2 * s + 1];
+                    const float ca = conic4[4 * s], cb = conic4[4 * s + 1], cc = conic4[4 * s + 2];
+                    const float o = color4[4 * s + 3];
+                    const float det = ca * cc - cb * cb;
+                    float ex, ey;
+                    if (!(o > kGsoCullAlpha)) continue;
+                    if (!(det > 0.0f) || !(ca > 0.0f) || !(cc > 0.0f)) {
+                        ex = ey = 1e30f;
+                    } else {
+                        const float qc = 2.0f * logf(o / kGsoCullAlpha);
+                        ex = sqrtf(qc * cc / det);
+                        ey = sqrtf(qc * ca / det);
+                    }
+                    if (!(x - ex <= bx1 && x + ex >= bx0 && y - ey <= by1 && y + ey >= by0)) continue;
+                    e += 64;
+                    for (int p = 0; p < 64; ++p) {
+                        if (T[p] == 0.0f) continue;
+                        const float dx = ((float)(wx0 + (p & 7)) * texx - 1.0f) - x;
+                        const float dy = ((float)(wy0 + (p >> 3)) * texy - 1.0f) - y;
+                        const float q = ca * dx * dx + cc * dy * dy + 2.0f * cb * dx * dy;
+                        float a = o * expf(-0.5f * q);
+                        a = a > 1.0f ? 1.0f : (a < 0.0f ? 0.0f : a);
+                        T[p] -= T[p] * a;
+                        if (T[p] < t_min) T[p] = 0.0f;
+                    }
+                }
+                live = 0;
+                for (int p = 0; p < 64; ++p) live += T[p] > 0.0f;
+            }
+        }
+    return e;
+}
+
 void gso_raster(const gso_camera* cam, const gso_cfg* cfg, const int32_t* ranges, const int32_t* values,
                 const float* xy, const float* conic4, const float* color4, uint8_t* rgba, int64_t* evals)
 {
@@ -679,13 +752,17 @@ void gso_raster(const gso_camera* cam, const gso_cfg* cfg, const int32_t* ranges
     const int tw = cfg->tile_w, th = cfg->tile_h, np = tw * th;
     const float texx = 2.0f / (float)W, texy = 2.0f / (float)H;
     const int ntiles = g.tiles_x * g.tiles_y;
-    int64_t total_evals = 0;
-#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total_evals)
+    int64_t total_evals = 0, block_evals = 0;
+    const int count_blocks = g_count_blocks && cfg->termination == 1 && tw % 8 == 0 && th % 8 == 0;
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : total_evals, block_evals)
     for (int tile = 0; tile < ntiles; ++tile) {
         int32_t first = ranges[2 * tile], last = ranges[2 * tile + 1];
         int count = last - first;
         if (count == 0) continue;
         int tx = tile % g.tiles_x, ty = tile / g.tiles_x;
+        if (count_blocks)
+            block_evals += block_walk_evals(tx * tw, ty * th, tw, th, W, H, texx, texy, values + first, count, xy,
+                                            conic4, color4, cfg->t_min);
         float T[1024], C[1024][3], pcx[1024], pcy[1024];
         int inimg[1024], done[1024];
         for (int p = 0; p < np; ++p) {
@@ -757,6 +834,7 @@ void gso_raster(const gso_camera* cam, const gso_cfg* cfg, const int32_t* ranges
         }
     }
     if (evals) *evals = total_evals;
+    if (count_blocks) g_block_evals += block_evals;
 }
 
 /* ---- whole frame --------------------------------------------------------- */

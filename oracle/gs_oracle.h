@@ -100,6 +100,12 @@ void gso_ranges(int64_t k, const uint64_t* keys, int32_t num_tiles, int32_t* ran
 /* Tile rasteriser (core/gaussian_render.cu:679-759).  rgba[4*W*H] must be
  * pre-cleared by the caller.  If evals != NULL it receives the number of
  * (pixel, splat) blend evaluations executed. */
+/* When on (reset to 0 by the call), gso_raster in T_min mode also adds to a
+ * counter the (pixel, entry) evaluations that the GPU's warp-culled raster
+ * executes (8x8 blocks, 32-entry chunks, cutoff alpha 2^-18); read it with
+ * gso_block_evals. */
+void gso_set_count_block_evals(int on);
+int64_t gso_block_evals(void);
 void gso_raster(const gso_camera* cam, const gso_cfg* cfg, const int32_t* ranges, const int32_t* values,
                 const float* xy, const float* conic4, const float* color4, uint8_t* rgba, int64_t* evals);
 

@@ -217,3 +217,26 @@ def test_tile_counts_consistent_with_build(O, gs):
     same = np.diff(vals) == 0
     assert (np.diff(tiles)[same] > 0).all()
     assert tiles.max() < gs.num_tiles(640, 480, rc)
+
+
+def test_block_eval_count_of_the_warp_culled_raster(O, gs):
+    """The oracle's count of the evaluations the GPU's warp-culled T_min
+    raster executes: counting leaves the image and the unculled count
+    unchanged; an 8x8 block evaluates each kept entry for all 64 pixels;
+    reference-mode frames add nothing."""
+    sc = gs.scenes.uniform_scene(5000, seed=9)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    cam = gs.look_at((0.2, 0.1, 3.0), (0, 0, 0), (0, 1, 0), 60.0, 160, 120, 0.1, 100.0)
+    rc = gs.RenderConfig()
+    img0, k0, ev0, _ = O.render(sc, sh, cam, rc)
+    O.count_block_evals(True)
+    img1, k1, ev1, _ = O.render(sc, sh, cam, rc)
+    blocks = O.block_evals()
+    O.count_block_evals(False)
+    assert np.array_equal(img0, img1) and k0 == k1 and ev0 == ev1
+    assert blocks > 0 and blocks % 64 == 0
+    # reference-mode frames are not counted
+    O.count_block_evals(True)
+    O.render(sc, sh, cam, gs.RenderConfig.reference())
+    assert O.block_evals() == 0
+    O.count_block_evals(False)
