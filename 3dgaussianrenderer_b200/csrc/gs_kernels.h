@@ -139,11 +139,14 @@ struct EmitArgs {
 };
 
 // Raster record of one (view, Gaussian) for GS_TERM_TMIN, written by the
-// frame kernel: the exponent of the splat's density at an offset (dx, dy)
-// is p = A dx^2 + B dx dy + C dy^2 (the conic scaled by -log2(e)/2, so
-// density = exp2(p)), and the cull extents bound the ellipse where
-// opacity * density = kCullAlpha.
-//   r0 = (x, y, A, B)   r1 = (C, opacity, red, green)   r2 = (blue, ext_x, ext_y, 0)
+// frame kernel: alpha at an offset (dx, dy) from the centre is
+// 2^(A dx^2 + B dx dy + C dy^2 + L) -- the conic scaled by -log2(e)/2 and
+// L = log2(opacity), so alpha = opacity * exp(-q/2) with one exp2 -- and
+// the cull extents bound the ellipse where alpha = kCullAlpha.  A record
+// whose conic is not positive definite (non-finite projections) has
+// L = -1e30 and empty extents: it contributes nothing, as the reference's
+// saturate(NaN) = 0 makes it.
+//   r0 = (x, y, A, B)   r1 = (C, L, red, green)   r2 = (blue, ext_x, ext_y, 0)
 constexpr float kCullAlpha = 3.814697265625e-06f;  // 2^-18
 
 // Onesweep LSD radix sort of (uint64 key, int32 value) pairs.  Tiles of

@@ -312,19 +312,22 @@ __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(Fr
                     a.color[o] = col;
                     a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
                 } else {
-                    a.rec[3 * o + 0] = make_float4(s.x, s.y, -0.72134752f * s.ca, -1.44269504f * s.cb);
-                    float ex, ey;
+                    float ex, ey, A = -0.72134752f * s.ca, B = -1.44269504f * s.cb, C = -0.72134752f * s.cc;
+                    float L = log2f(col.w);
                     const float det = s.ca * s.cc - s.cb * s.cb;
-                    if (!(col.w > kCullAlpha)) {
-                        ex = ey = -1e30f;  // contributes nothing anywhere
-                    } else if (!(det > 0.0f) || !(s.ca > 0.0f) || !(s.cc > 0.0f)) {
-                        ex = ey = 1e30f;  // degenerate conic: never culled
+                    if (!(det > 0.0f) || !(s.ca > 0.0f) || !(s.cc > 0.0f) || !(col.w > kCullAlpha)) {
+                        // contributes nothing anywhere: alpha below the cutoff,
+                        // or a conic that is not positive definite
+                        ex = ey = -1e30f;
+                        A = B = C = 0.0f;
+                        L = -1e30f;
                     } else {
                         const float qc = 2.0f * logf(col.w / kCullAlpha);
                         ex = sqrtf(qc * s.cc / det);
                         ey = sqrtf(qc * s.ca / det);
                     }
-                    a.rec[3 * o + 1] = make_float4(-0.72134752f * s.cc, col.w, col.x, col.y);
+                    a.rec[3 * o + 0] = make_float4(s.x, s.y, A, B);
+                    a.rec[3 * o + 1] = make_float4(C, L, col.x, col.y);
                     a.rec[3 * o + 2] = make_float4(col.z, ex, ey, 0.0f);
                 }
             }

@@ -456,25 +456,19 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
 // survivors are packed in list order into per-warp shared-memory slots
 // (rank = popcount of the ballot below the lane) and every lane blends them
 // into both its pixels as one packed f32x2 pair.  The column terms of the
-// exponent (A dx^2, B dx) are formed once per lane in scalar arithmetic;
-// the pair shares them.  A warp stops when all its pixels are done.
-// Blend per pixel: p = A dx^2 + B dx dy + C dy^2, alpha = sat(opacity 2^p)
-// (= opacity 2^p for the positive definite conics that make p <= 0),
-// w = T alpha, colour += rgb w, T -= w; a pixel whose T falls below t_min
-// is done: its T is set to 0, so every later w is exactly 0 and its colour
-// no longer changes.
+// exponent (A dx^2 + L, B dx) are formed once per lane in scalar
+// arithmetic; the pair shares them.
+// Blend per pixel: alpha = 2^(A dx^2 + B dx dy + C dy^2 + L) (opacity
+// folded in as L = log2(opacity); the conics are positive definite, so
+// alpha <= opacity), w = T alpha, colour += rgb w, T -= w.  A warp stops
+// after the chunk in which all its pixels reached T < t_min; a pixel that
+// got there earlier keeps blending until then, which adds less than t_min
+// to its colour (the w that follow sum to less than its T).
 
 __device__ __forceinline__ float ex2_approx(const float x)
 {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-__device__ __forceinline__ float mul_sat(const float a, const float b)
-{
-    float y;
-    asm("mul.rn.sat.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
     return y;
 }
 
@@ -569,26 +563,22 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
             const ulonglong2 yc = s_yc[warp][k];
             const ulonglong2 rg = s_rg[warp][k];
             const float dx = cx - e.x;
-            const f2 adx2 = f2_dup(e.y * dx * dx);
+            const f2 adx2 = f2_dup(fmaf(e.y * dx, dx, e.w));  // A dx^2 + L
             const f2 bdx = f2_dup(e.z * dx);
             const f2 dyy = f2_sub(cyy, yc.x);
             const f2 p = f2_fma(f2_fma(yc.y, dyy, bdx), dyy, adx2);
             float p0, p1;
             f2_unpack(p, p0, p1);
-            const f2 w = f2_mul(TT, f2_pack(mul_sat(e.w, ex2_approx(p0)), mul_sat(e.w, ex2_approx(p1))));
+            const f2 w = f2_mul(TT, f2_pack(ex2_approx(p0), ex2_approx(p1)));
             R = f2_fma(rg.x, w, R);
             G = f2_fma(rg.y, w, G);
             B = f2_fma(s_bl[warp][k], w, B);
-            float T0, T1;
-            f2_unpack(f2_sub(TT, w), T0, T1);
-            T0 = T0 < tmin ? 0.0f : T0;
-            T1 = T1 < tmin ? 0.0f : T1;
-            TT = f2_pack(T0, T1);
+            TT = f2_sub(TT, w);
         }
         __syncwarp();  // slots are rewritten by the next chunk
         float T0, T1;
         f2_unpack(TT, T0, T1);
-        done = T0 == 0.0f && T1 == 0.0f;
+        done = T0 < tmin && T1 < tmin;
     }
     float r0, r1, g0, g1, b0, b1;
     f2_unpack(R, r0, r1);

@@ -705,7 +705,7 @@ static int64_t block_walk_evals(int tile_px0, int tile_py0, int tw, int th, int 
             for (int p = 0; p < 64; ++p) {
                 const int px = wx0 + (p & 7), py = wy0 + (p >> 3);
                 T[p] = (px < W && py < H) ? 1.0f : 0.0f;
-                live += T[p] > 0.0f;
+                live += T[p] >= t_min;
             }
             for (int c0 = 0; c0 < count && live; c0 += 32) {
                 const int nb = count - c0 < 32 ? count - c0 : 32;
@@ -715,30 +715,24 @@ static int64_t block_walk_evals(int tile_px0, int tile_py0, int tw, int th, int 
                     const float ca = conic4[4 * s], cb = conic4[4 * s + 1], cc = conic4[4 * s + 2];
                     const float o = color4[4 * s + 3];
                     const float det = ca * cc - cb * cb;
-                    float ex, ey;
-                    if (!(o > kGsoCullAlpha)) continue;
-                    if (!(det > 0.0f) || !(ca > 0.0f) || !(cc > 0.0f)) {
-                        ex = ey = 1e30f;
-                    } else {
-                        const float qc = 2.0f * logf(o / kGsoCullAlpha);
-                        ex = sqrtf(qc * cc / det);
-                        ey = sqrtf(qc * ca / det);
-                    }
+                    /* below the cutoff, or a conic that is not positive definite: no record */
+                    if (!(o > kGsoCullAlpha) || !(det > 0.0f) || !(ca > 0.0f) || !(cc > 0.0f)) continue;
+                    const float qc = 2.0f * logf(o / kGsoCullAlpha);
+                    const float ex = sqrtf(qc * cc / det), ey = sqrtf(qc * ca / det);
                     if (!(x - ex <= bx1 && x + ex >= bx0 && y - ey <= by1 && y + ey >= by0)) continue;
                     e += 64;
                     for (int p = 0; p < 64; ++p) {
-                        if (T[p] == 0.0f) continue;
+                        if (T[p] < t_min) continue;
                         const float dx = ((float)(wx0 + (p & 7)) * texx - 1.0f) - x;
                         const float dy = ((float)(wy0 + (p >> 3)) * texy - 1.0f) - y;
                         const float q = ca * dx * dx + cc * dy * dy + 2.0f * cb * dx * dy;
                         float a = o * expf(-0.5f * q);
                         a = a > 1.0f ? 1.0f : (a < 0.0f ? 0.0f : a);
                         T[p] -= T[p] * a;
-                        if (T[p] < t_min) T[p] = 0.0f;
                     }
                 }
                 live = 0;
-                for (int p = 0; p < 64; ++p) live += T[p] > 0.0f;
+                for (int p = 0; p < 64; ++p) live += T[p] >= t_min;
             }
         }
     return e;
