@@ -113,6 +113,9 @@ struct FrameGraph {
     int failed = 0;                  // capture failed: run this key without a graph
 };
 constexpr size_t kMaxGraphs = 8;
+// gs_render_batch_host renders batches of more than this many views in
+// chunks, reading each chunk back while the next one renders.
+constexpr int kHostChunkViews = 16;
 
 std::atomic<uint64_t> g_scene_uid{1};
 
@@ -153,6 +156,7 @@ struct gs_ctx {
     int64_t key_capacity = 0;
     int64_t per_view_capacity = 0;         // Gaussians * views the splat buffers hold
     cudaStream_t cap_stream = nullptr;     // graph capture
+    cudaStream_t copy_stream = nullptr;    // image read-back of the host-output batches
     bool tile_count_dirty = true;          // tile counts may be nonzero: clear before the next frame
     std::vector<FrameGraph> graphs;
     uint64_t use_clock = 0;
@@ -802,8 +806,9 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
         stats->num_keys = ctx->h_counters->total;
         stats->num_tiles = p.tiles_total;
-        // frame kernel, tile scan, bucket emit, big-tile sort, raster (sorts the other tiles)
-        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 2;
+        // frame kernel, bucket emit, big-tile sort; tile scan, tile order,
+        // raster (sorts the other tiles)
+        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 3;
         stats->graph_replay = replayed ? 1 : 0;
         stats->attempts = attempts;
     }
@@ -938,6 +943,7 @@ int gs_ctx_destroy(gs_ctx* ctx)
     for (FrameGraph& g : ctx->graphs) drop_graph(g);
     ctx->graphs.clear();
     if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+    if (ctx->copy_stream) cudaStreamDestroy(ctx->copy_stream);
     DevBuf* bufs[] = {&ctx->views, &ctx->color, &ctx->xy, &ctx->z, &ctx->ell, &ctx->conic, &ctx->rect,
                       &ctx->offsets, &ctx->rec, &ctx->hitmask, &ctx->scan_status, &ctx->view_stats, &ctx->keys0, &ctx->vals0, &ctx->keys1, &ctx->vals1,
                       &ctx->sort_hist, &ctx->sort_status, &ctx->ranges, &ctx->tile_count, &ctx->cursor, &ctx->big_list, &ctx->tile_order,
@@ -1179,10 +1185,48 @@ int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* ca
     std::vector<uint8_t*> outs((size_t)num_views);
     for (int v = 0; v < num_views; ++v) outs[v] = ctx->image.as<uint8_t>() + offs[v];
     cudaStream_t st = (cudaStream_t)stream;
-    int rc = run_frame(ctx, scene, cams, num_views, *cfg, outs.data(), stats, st);
+    if (num_views <= kHostChunkViews) {
+        int rc = run_frame(ctx, scene, cams, num_views, *cfg, outs.data(), stats, st);
+        if (rc) return rc;
+        GS_CUDA(cudaMemcpyAsync(h_rgba, ctx->image.p, total, cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        return GS_OK;
+    }
+    // Larger batches render in chunks of kHostChunkViews views; each chunk's
+    // images are copied to the host on a second stream while the next chunk
+    // renders (a frame returns with its stream synchronised, so the chunk is
+    // complete when its copy is queued).  The frame kernel reads the scene
+    // once per 16 views anyway, so the chunks cost little batching.
+    if (!ctx->copy_stream) GS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    gs_stats acc{};
+    acc.graph_replay = 1;
+    int rc = GS_OK;
+    for (int c0 = 0; c0 < num_views && rc == GS_OK; c0 += kHostChunkViews) {
+        const int nv = std::min(kHostChunkViews, num_views - c0);
+        gs_stats sc{};
+        rc = run_frame(ctx, scene, cams + c0, nv, *cfg, outs.data() + c0, &sc, st);
+        if (rc) break;
+        const size_t end = c0 + nv < num_views ? offs[c0 + nv] : total;
+        const cudaError_t e = cudaMemcpyAsync(h_rgba + offs[c0], outs[c0], end - offs[c0], cudaMemcpyDeviceToHost,
+                                              ctx->copy_stream);
+        if (e != cudaSuccess) rc = cuda_fail(e, "image copy");
+        acc.sh_eval_ms += sc.sh_eval_ms;
+        acc.project_ms += sc.project_ms;
+        acc.build_tile_ms += sc.build_tile_ms;
+        acc.sort_ms += sc.sort_ms;
+        acc.raster_ms += sc.raster_ms;
+        acc.total_ms += sc.total_ms;
+        acc.num_keys += sc.num_keys;
+        acc.num_tiles += sc.num_tiles;
+        acc.kernel_launches += sc.kernel_launches;
+        acc.graph_replay = acc.graph_replay && sc.graph_replay;
+        acc.attempts = std::max(acc.attempts, sc.attempts);
+    }
+    // the copies already queued finish before the call returns, also on an error
+    const cudaError_t se = cudaStreamSynchronize(ctx->copy_stream);
     if (rc) return rc;
-    GS_CUDA(cudaMemcpyAsync(h_rgba, ctx->image.p, total, cudaMemcpyDeviceToHost, st));
-    GS_CUDA(cudaStreamSynchronize(st));
+    if (se != cudaSuccess) return cuda_fail(se, "image copy");
+    if (stats) *stats = acc;
     return GS_OK;
 }
 

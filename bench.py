@@ -332,7 +332,9 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_e2e:
         host = torch.empty(total_bytes, dtype=torch.uint8).pin_memory()
         host_np = host.numpy()
-        for _ in range(max(1, args.warmup // 2)):
+        # a frame is captured into a CUDA graph on its second call: warm up
+        # past that, as for the device-output leg
+        for _ in range(max(3, args.warmup)):
             gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
         torch.cuda.synchronize()
         if world > 1:

@@ -240,6 +240,36 @@ def test_batch_views_identical_to_single(gs, ctx):
         off += size
 
 
+@pytest.mark.parametrize("views", [17, 40])
+def test_large_host_batch_chunks_match_device_batch(gs, ctx, views):
+    """Host-output batches above 16 views render 16 views at a time with the
+    read-back overlapped; every image equals the device-output batch's (one
+    frame for all views), the stats add up the chunks."""
+    torch = pytest.importorskip("torch")
+    sc = gs.scenes.cluster_scene(120_000, 32, 5.0, seed=78)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    rng = np.random.default_rng(6)
+    sizes = [(1280, 720), (640, 480), (800, 600)]
+    cams = [gs.look_at(gs.scenes.sphere_pose(rng, 12.0), (0, 0, 0), (0, 1, 0), 50.0, *sizes[i % 3], 0.1, 100.0)
+            for i in range(views)]
+    for rc in (gs.RenderConfig(), gs.RenderConfig.reference()):
+        outs = [torch.zeros((c.GetHeight(), c.GetWidth(), 4), dtype=torch.uint8, device="cuda") for c in cams]
+        std = gs.render_batch(ctx, scene, cams, rc, outs)
+        torch.cuda.synchronize()
+        total = sum(c.GetWidth() * c.GetHeight() * 4 for c in cams)
+        host = np.zeros(total, np.uint8)
+        sth = gs.render_batch_host(ctx, scene, cams, rc, host)
+        assert sth["num_keys"] == std["num_keys"]
+        assert sth["num_tiles"] == std["num_tiles"]
+        off = 0
+        for c, o in zip(cams, outs):
+            size = c.GetWidth() * c.GetHeight() * 4
+            assert np.array_equal(host[off:off + size].reshape(c.GetHeight(), c.GetWidth(), 4), o.cpu().numpy())
+            off += size
+    scene.close()
+
+
 @pytest.mark.parametrize("n", [0, 1, 31, 32, 33, 257, 4097])
 def test_small_and_empty_scenes(gs, ctx, O, n):
     sc = gs.scenes.uniform_scene(max(n, 1), seed=n + 3)
