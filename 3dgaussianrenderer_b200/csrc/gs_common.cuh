@@ -80,6 +80,34 @@ struct Splat {
     float ca, cb, cc;   // conic
 };
 
+// Approximate PTX arithmetic for the T_min frames' projection (FAST): the
+// hardware reciprocal, square root and reciprocal square root (a few ulp),
+// where the reference-compatible path keeps IEEE division and sqrtf.
+__device__ __forceinline__ float rcp_approx(const float x)
+{
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float sqrt_approx(const float x)
+{
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rsqrt_approx(const float x)
+{
+    float y;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float lg2_approx(const float x)
+{
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 // View position and clip-space centre of one Gaussian (the first half of
 // the projection, gaussian_render.cu:160-182): enough to decide the
 // frustum test, so Gaussians outside the view can skip the rest.
@@ -90,6 +118,7 @@ struct ViewPos {
     float cx, cy, cz;                  // clip space, before the cull
 };
 
+template <bool FAST = false>
 __device__ __forceinline__ ViewPos view_position(const float4 p, const ViewParams& v)
 {
     ViewPos w;
@@ -100,7 +129,10 @@ __device__ __forceinline__ ViewPos view_position(const float4 p, const ViewParam
     w.vy = (V[1] * p.x + V[5] * p.y) + (V[9] * p.z + V[13] * 1.0f);
     w.vz = (V[2] * p.x + V[6] * p.y) + (V[10] * p.z + V[14] * 1.0f);
 
-    w.zRcp = 1.0f / w.vz;
+    if constexpr (FAST)
+        w.zRcp = rcp_approx(w.vz);
+    else
+        w.zRcp = 1.0f / w.vz;
     w.zRcpSqr = w.zRcp * w.zRcp;
     w.scaleX = -v.cot[0] * w.zRcp;
     w.scaleY = -v.cot[1] * w.zRcp;
@@ -131,7 +163,11 @@ __device__ __forceinline__ bool in_frustum(const ViewPos& w)
 // EWA projection of one Gaussian: quaternion decode, covariance
 // R S S^T R^T, affine Jacobian of the perspective divide, clip-space 2x2
 // covariance plus trace bump, eigen-decomposition, conic and frustum test.
-// `w` is view_position(p, v).
+// `w` is view_position(p, v).  FAST (the T_min frames, whose geometry
+// need not match the reference bit for bit): hardware reciprocal and square
+// roots, and the ellipse axis taken from the normalised eigenvector itself
+// instead of cos/sin of its atan2 angle, which is the same vector.
+template <bool FAST = false>
 __device__ __forceinline__ Splat project_gaussian(const ViewPos& w, const float4 sr, const ViewParams& v)
 {
     const uint32_t bits = __float_as_uint(sr.w);
@@ -194,20 +230,20 @@ __device__ __forceinline__ Splat project_gaussian(const ViewPos& w, const float4
     const float det = c00 * c11 - c10 * c10;
     const float mid = 0.5f * (c00 + c11);
     constexpr float eps = 1e-12f;
-    const float radius = sqrtf(gmax(eps, mid * mid - det));
+    const float r2 = gmax(eps, mid * mid - det);
+    const float radius = FAST ? sqrt_approx(r2) : sqrtf(r2);
     const float lambda0 = mid + radius;
     const float lambda1 = gmax(0.0f, mid - radius);
 
     // normalize(vec2(c10, lambda0 - c00)) = v * (1 / sqrt(dot(v, v)))
     float e0x = c10, e0y = lambda0 - c00;
     const float dd = e0x * e0x + e0y * e0y;
-    const float inv = 1.0f / sqrtf(dd);
+    const float inv = FAST ? rsqrt_approx(dd) : 1.0f / sqrtf(dd);
     e0x = e0x * inv;
     e0y = e0y * inv;
-    const float angle = atan2f(e0y, e0x);
-    float ex = sqrtf(lambda0) * 3.0f;
-    float ey = sqrtf(lambda1) * 3.0f;
-    const float invDet = 1.0f / gmax(eps, det);
+    float ex = (FAST ? sqrt_approx(lambda0) : sqrtf(lambda0)) * 3.0f;
+    float ey = (FAST ? sqrt_approx(lambda1) : sqrtf(lambda1)) * 3.0f;
+    const float invDet = FAST ? rcp_approx(gmax(eps, det)) : 1.0f / gmax(eps, det);
 
     // step(-1, clip) * step(clip, 1) * step(0, lambda1)   (:205-206)
     const float edgex = (cx < -1.0f ? 0.0f : 1.0f) * (1.0f < cx ? 0.0f : 1.0f);
@@ -226,8 +262,14 @@ __device__ __forceinline__ Splat project_gaussian(const ViewPos& w, const float4
     s.x = cx;
     s.y = cy;
     s.z = cz;
-    s.cs = cosf(angle);
-    s.sn = sinf(angle);
+    if constexpr (FAST) {
+        s.cs = e0x;
+        s.sn = e0y;
+    } else {
+        const float angle = atan2f(e0y, e0x);
+        s.cs = cosf(angle);
+        s.sn = sinf(angle);
+    }
     s.ex = ex;
     s.ey = ey;
     s.ca = c11 * invDet;

@@ -216,7 +216,7 @@ __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
 // blocks are independent and run in launch order.
 // Blocks per SM: SH degree 3 keeps 80 registers (3 blocks); lower degrees
 // run faster at 4 blocks (64 registers)
-template <int DEG, bool BUCKET>
+template <int DEG, bool BUCKET, bool FAST>
 __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(FrameArgs a)
 {
     extern __shared__ __align__(128) float s_sh[];  // [3*(DEG+1)^2][256]
@@ -269,9 +269,9 @@ __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(Fr
         if (valid) {
             // outside the frustum: culled, no tile (whole warps of a
             // spatially ordered scene skip the projection together)
-            const ViewPos w = view_position(p, v);
+            const ViewPos w = view_position<FAST>(p, v);
             if (in_frustum(w)) {
-                s = project_gaussian(w, sr, v);
+                s = project_gaussian<FAST>(w, sr, v);
                 e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
                 r = tile_rect(e, v);
                 cand = rect_candidates(r);
@@ -313,7 +313,7 @@ __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(Fr
                     a.conic[o] = make_float4(s.ca, s.cb, s.cc, 0.0f);
                 } else {
                     float ex, ey, A = -0.72134752f * s.ca, B = -1.44269504f * s.cb, C = -0.72134752f * s.cc;
-                    float L = log2f(col.w);
+                    float L = lg2_approx(col.w);
                     const float det = s.ca * s.cc - s.cb * s.cb;
                     if (!(det > 0.0f) || !(s.ca > 0.0f) || !(s.cc > 0.0f) || !(col.w > kCullAlpha)) {
                         // contributes nothing anywhere: alpha below the cutoff,
@@ -322,9 +322,12 @@ __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(Fr
                         A = B = C = 0.0f;
                         L = -1e30f;
                     } else {
-                        const float qc = 2.0f * logf(col.w / kCullAlpha);
-                        ex = sqrtf(qc * s.cc / det);
-                        ey = sqrtf(qc * s.ca / det);
+                        // qc = 2 ln(opacity / cutoff) = 2 ln 2 (L + 18); 1.0001
+                        // covers the approximations
+                        const float qc = 1.38643f * (L + 18.0f);
+                        const float rdet = rcp_approx(det);
+                        ex = sqrt_approx(qc * s.cc * rdet);
+                        ey = sqrt_approx(qc * s.ca * rdet);
                     }
                     a.rec[3 * o + 0] = make_float4(s.x, s.y, A, B);
                     a.rec[3 * o + 1] = make_float4(C, L, col.x, col.y);
@@ -501,38 +504,46 @@ void launch_project_stage(int64_t n, const float4* pos, const float4* sr, const 
     project_stage_kernel<<<grid, 256, 0, st>>>(n, pos, sr, v, xy, z, ell, conic);
 }
 
-template <int DEG, bool BUCKET>
+template <int DEG, bool BUCKET, bool FAST>
 static void launch_frame_deg(const FrameArgs& a, cudaStream_t st)
 {
     constexpr int NCOEF = DEG >= 0 ? 3 * (DEG + 1) * (DEG + 1) : 0;
     constexpr int smem = NCOEF * 256 * (int)sizeof(float);
     static bool attr = false;
     if (!attr) {
-        cudaFuncSetAttribute(frame_project_kernel<DEG, BUCKET>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+        cudaFuncSetAttribute(frame_project_kernel<DEG, BUCKET, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem);
         attr = true;
     }
-    frame_project_kernel<DEG, BUCKET><<<(unsigned)a.num_tiles, 256, smem, st>>>(a);
+    frame_project_kernel<DEG, BUCKET, FAST><<<(unsigned)a.num_tiles, 256, smem, st>>>(a);
 }
 
-template <bool BUCKET>
+template <bool BUCKET, bool FAST>
 static void launch_frame_mode(const FrameArgs& a, int deg, cudaStream_t st)
 {
     switch (deg) {
-        case -1: launch_frame_deg<-1, BUCKET>(a, st); break;
-        case 0: launch_frame_deg<0, BUCKET>(a, st); break;
-        case 1: launch_frame_deg<1, BUCKET>(a, st); break;
-        case 2: launch_frame_deg<2, BUCKET>(a, st); break;
-        default: launch_frame_deg<3, BUCKET>(a, st); break;
+        case -1: launch_frame_deg<-1, BUCKET, FAST>(a, st); break;
+        case 0: launch_frame_deg<0, BUCKET, FAST>(a, st); break;
+        case 1: launch_frame_deg<1, BUCKET, FAST>(a, st); break;
+        case 2: launch_frame_deg<2, BUCKET, FAST>(a, st); break;
+        default: launch_frame_deg<3, BUCKET, FAST>(a, st); break;
     }
 }
 
+// T_min frames (raster records) project with the approximate arithmetic,
+// reference-compatible frames with the exact one, in both orderings.
 void launch_frame_project(const FrameArgs& a, int deg, cudaStream_t st, bool bucket)
 {
     if (a.num_tiles == 0) return;
-    if (bucket)
-        launch_frame_mode<true>(a, deg, st);
+    const bool fast = a.raster_mode != 0;
+    if (bucket && fast)
+        launch_frame_mode<true, true>(a, deg, st);
+    else if (bucket)
+        launch_frame_mode<true, false>(a, deg, st);
+    else if (fast)
+        launch_frame_mode<false, true>(a, deg, st);
     else
-        launch_frame_mode<false>(a, deg, st);
+        launch_frame_mode<false, false>(a, deg, st);
 }
 
 void launch_count_stage(const FrameArgs& a, cudaStream_t st)
