@@ -146,7 +146,8 @@ struct EmitArgs {
 // whose conic is not positive definite (non-finite projections) has
 // L = -1e30 and empty extents: it contributes nothing, as the reference's
 // saturate(NaN) = 0 makes it.
-//   r0 = (x, y, A, B)   r1 = (C, L, red, green)   r2 = (blue, ext_x, ext_y, 0)
+//   r0 = (x, y, ext_x, ext_y)   r1 = (A, B, C, L)   r2 = (red, green, blue, 0)
+// (the cull test reads r0 only; r1 and r2 are read for the kept entries)
 constexpr float kCullAlpha = 3.814697265625e-06f;  // 2^-18
 
 // Onesweep LSD radix sort of (uint64 key, int32 value) pairs.  Tiles of

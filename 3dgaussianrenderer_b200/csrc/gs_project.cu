@@ -329,9 +329,9 @@ __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(Fr
                         ex = sqrt_approx(qc * s.cc * rdet);
                         ey = sqrt_approx(qc * s.ca * rdet);
                     }
-                    a.rec[3 * o + 0] = make_float4(s.x, s.y, A, B);
-                    a.rec[3 * o + 1] = make_float4(C, L, col.x, col.y);
-                    a.rec[3 * o + 2] = make_float4(col.z, ex, ey, 0.0f);
+                    a.rec[3 * o + 0] = make_float4(s.x, s.y, ex, ey);
+                    a.rec[3 * o + 1] = make_float4(A, B, C, L);
+                    a.rec[3 * o + 2] = make_float4(col.x, col.y, col.z, 0.0f);
                 }
             }
         }

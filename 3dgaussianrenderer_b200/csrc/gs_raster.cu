@@ -537,23 +537,23 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
         if (__all_sync(kFull, done)) break;
         const int j = base + lane;
         bool keep = false;
-        float4 q0, q2;
+        float4 q0;
         const float4* rp = nullptr;
         if (j < last) {
             const int s = slot_at(a, sk, first, j - first);
             rp = a.rec + 3 * (int64_t)s;
-            q0 = __ldg(rp);
-            q2 = __ldg(rp + 2);
-            keep = (q0.x - q2.y <= bx1) && (q0.x + q2.y >= bx0) && (q0.y - q2.z <= by1) && (q0.y + q2.z >= by0);
+            q0 = __ldg(rp);  // (x, y, ext_x, ext_y)
+            keep = (q0.x - q0.z <= bx1) && (q0.x + q0.z >= bx0) && (q0.y - q0.w <= by1) && (q0.y + q0.w >= by0);
         }
         const unsigned bal = __ballot_sync(kFull, keep);
         if (keep) {
             const int k = __popc(bal & lt);
-            const float4 q1 = __ldg(rp + 1);
-            s_s[warp][k] = make_float4(q0.x, q0.z, q0.w, q1.y);
-            s_yc[warp][k] = make_ulonglong2(f2_dup(q0.y), f2_dup(q1.x));
-            s_rg[warp][k] = make_ulonglong2(f2_dup(q1.z), f2_dup(q1.w));
-            s_bl[warp][k] = f2_dup(q2.x);
+            const float4 q1 = __ldg(rp + 1);  // (A, B, C, L)
+            const float4 q2 = __ldg(rp + 2);  // (red, green, blue, 0)
+            s_s[warp][k] = make_float4(q0.x, q1.x, q1.y, q1.w);
+            s_yc[warp][k] = make_ulonglong2(f2_dup(q0.y), f2_dup(q1.z));
+            s_rg[warp][k] = make_ulonglong2(f2_dup(q2.x), f2_dup(q2.y));
+            s_bl[warp][k] = f2_dup(q2.z);
         }
         __syncwarp();  // slot writes visible to the whole warp
         const int cnt = __popc(bal);
