@@ -206,6 +206,20 @@ def run_serving(gs, rank, rate=500.0, duration_s=3.0, budget_gb=150, max_batch=1
             "scenes_m": [n / 1e6 for n in SERVE_SCENES]}
 
 
+def job_views_per_s(local_ms: float, views_per_rank: int, steps: int, world: int, device=None) -> tuple:
+    """Whole-job throughput of `world` replicas: every rank renders its own
+    views (no exchange), the job takes as long as the slowest rank, so
+    value = all ranks' views / max over ranks of the timed milliseconds.
+    Returns (value, max_ms); a collective only when world > 1."""
+    import torch
+    t = torch.tensor([float(local_ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return world * views_per_rank * steps / (ms_max / 1e3), ms_max
+
+
 def run_ref1024(gs, ctx, sc, dev, stream, frames=30):
     """The single-view path in reference-compatible mode (SH degree <= 2 as
     the reference evaluates it, tile-wide T <= 0.02 termination) on the same
@@ -320,11 +334,7 @@ def run_ours(args, rank, world, local_rank):
         clk.mark_end()
     ms = e0.elapsed_time(e1)
     clocks = clk.stop() if clk else None
-    t = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * VIEWS * args.steps / (ms_max / 1e3)
+    value, ms_max = job_views_per_s(ms, VIEWS, args.steps, world, dev)
 
     # e2e through the public host-buffer API: camera upload + images back to pinned host memory
     total_bytes = sum(c.GetWidth() * c.GetHeight() * 4 for c in cams)
@@ -346,10 +356,7 @@ def run_ours(args, rank, world, local_rank):
             gs.render_batch_host(ctx, scene, cams, rc, host_np, stream)
         f1.record(stream)
         torch.cuda.synchronize()
-        t = torch.tensor([f0.elapsed_time(f1)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_value = world * VIEWS * args.steps / (float(t.item()) / 1e3)
+        e2e_value, _ = job_views_per_s(f0.elapsed_time(f1), VIEWS, args.steps, world, dev)
 
     # plain single-view path over the same views (for the batched/plain ratio)
     plain_value = None
