@@ -120,6 +120,9 @@ _sig("gs_ctx_create", _I, _I, ctypes.POINTER(_P))
 _sig("gs_ctx_destroy", _I, _P)
 _sig("gs_ctx_device_bytes", _I64, _P)
 _sig("gs_scene_create", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.POINTER(_P))
+_sig("gs_draw_stats", _I, _P, _I32, _I32, _I64, ctypes.POINTER(gs_stats), ctypes.c_double, _P)
+_sig("gs_format_stats", _I, _I64, ctypes.POINTER(gs_stats), ctypes.c_double, ctypes.c_char_p, _I32)
+_sig("gs_font_glyph", _I, _I32, ctypes.POINTER(ctypes.c_uint8))
 _sig("gs_scene_create_ex", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.c_uint32, ctypes.POINTER(_P))
 _sig("gs_scene_destroy", _I, _P)
 _sig("gs_scene_size", _I64, _P)
@@ -423,6 +426,34 @@ def stage_sort(ctx: Context, num_keys, bits, d_keys, d_values, d_keys_alt, d_val
 
 def stage_ranges(num_keys, d_keys, tiles, d_ranges, stream=None):
     check(lib.gs_stage_ranges(num_keys, _ptr(d_keys), tiles, _ptr(d_ranges), _stream_ptr(stream)), "gs_stage_ranges")
+
+
+def _stats_struct(stats: dict) -> gs_stats:
+    st = gs_stats()
+    for name, _ in gs_stats._fields_:
+        if name in stats:
+            setattr(st, name, stats[name])
+    return st
+
+
+def draw_stats(d_rgba, width: int, height: int, num_gaussians: int, stats: dict, fps: float, stream=None):
+    """Performance overlay (DrawPerformanceOverlay) into a device RGBA8 image."""
+    st = _stats_struct(stats)
+    check(lib.gs_draw_stats(_ptr(d_rgba), width, height, num_gaussians, ctypes.byref(st), float(fps),
+                            _stream_ptr(stream)), "gs_draw_stats")
+
+
+def format_stats(num_gaussians: int, stats: dict, fps: float) -> str:
+    st = _stats_struct(stats)
+    buf = ctypes.create_string_buffer(1024)
+    check(lib.gs_format_stats(num_gaussians, ctypes.byref(st), float(fps), buf, len(buf)), "gs_format_stats")
+    return buf.value.decode()
+
+
+def font_glyph(c: str) -> list:
+    rows = (ctypes.c_uint8 * 7)()
+    check(lib.gs_font_glyph(ord(c), rows), "gs_font_glyph")
+    return list(rows)
 
 
 def stage_raster(cam: Camera, cfg: RenderConfig, d_ranges, d_values, d_xy, d_conic, d_color, d_rgba, stream=None):

@@ -165,6 +165,22 @@ GS_API int gs_render_batch(gs_ctx* ctx, const gs_scene* scene, const gs_camera* 
 GS_API int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
                          const gs_render_cfg* cfg, uint8_t* h_rgba, gs_stats* stats, void* stream);
 
+/* ---- performance overlay (app/perf_overlay.cpp:115-161) ---------------- */
+
+/* DrawPerformanceOverlay: draws the reference's eight statistics lines
+ * (FPS, Gaussians, Total, SH, Project, Build, Sort, Raster; same formats)
+ * as white 5x7-pixel text into the device RGBA8 image d_rgba (W x H, row 0
+ * at the bottom), upright and 5 pixels from the displayed image's top-left
+ * corner.  Asynchronous on `stream`; only the text pixels are written. */
+GS_API int gs_draw_stats(uint8_t* d_rgba, int32_t width, int32_t height, int64_t num_gaussians,
+                         const gs_stats* stats, double fps, void* stream);
+/* The eight lines gs_draw_stats draws, each ending in '\n', into `out`
+ * (NUL-terminated); GS_ERR_CAPACITY when `capacity` is too small. */
+GS_API int gs_format_stats(int64_t num_gaussians, const gs_stats* stats, double fps, char* out, int32_t capacity);
+/* The overlay font: 7 rows of glyph `c` (bit 4 = leftmost of 5 columns;
+ * all zero outside ASCII 32..126). */
+GS_API int gs_font_glyph(int32_t c, uint8_t rows[7]);
+
 /* ---- stage API (core/gaussian_render.cuh:113-126) ---------------------- */
 /* Explicit-argument replacements of the reference's constant-memory stage
  * functions.  All pointers are device pointers; every call is asynchronous

@@ -10,6 +10,7 @@
 //   gauss_render::Camera        core/camera.h:11-59 (+ GetFovY/GetZNear/GetZFar
 //                               that core/renderer.cpp:18,28 calls)
 //   gauss_render::Renderer      core/renderer.h:13-50
+//   gauss_render::DrawPerformanceOverlay  app/perf_overlay.h:9-15
 // Vector arguments accept any type with x/y/z members (glm::vec3 included).
 // Renderer::Render writes RGBA8 into a device buffer, like the reference's
 // mapped PBO (row 0 = bottom).  Errors are reported through the int
@@ -317,5 +318,21 @@ class Renderer {
     gs_scene* scene_ = nullptr;
     gs_render_cfg cfg_{};
 };
+
+// app/perf_overlay.h:9-15: the statistics text drawn into the image.  The
+// buffer is the device RGBA8 image Renderer::Render wrote (the reference's
+// is the mapped host PBO); asynchronous on `stream`.
+inline int DrawPerformanceOverlay(uint8_t* buffer, int width, int height, int num_gaussians, const RenderStats& stats,
+                                  double fps, void* stream = nullptr)
+{
+    gs_stats s{};
+    s.sh_eval_ms = stats.sh_eval_ms;
+    s.project_ms = stats.project_ms;
+    s.build_tile_ms = stats.build_tile_ms;
+    s.sort_ms = stats.sort_ms;
+    s.raster_ms = stats.raster_ms;
+    s.total_ms = stats.total_ms;
+    return gs_draw_stats(buffer, width, height, num_gaussians, &s, fps, stream);
+}
 
 }  // namespace gauss_render

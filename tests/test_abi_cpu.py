@@ -65,3 +65,23 @@ def test_errors_without_gpu(gs):
     # null arguments are rejected before any device work
     assert gs.lib.gs_render(None, None, None, None, None, None, None) == gs.GS_ERR_INVALID
     assert gs.lib.gs_stage_ranges(-1, None, 0, None, None) == gs.GS_ERR_INVALID
+
+
+def test_overlay_text_matches_reference_formats(gs):
+    """gs_format_stats formats the lines of DrawPerformanceOverlay
+    (app/perf_overlay.cpp:125-161) with the reference's formats."""
+    st = {"total_ms": 1.234, "sh_eval_ms": 0.0, "project_ms": 0.25, "build_tile_ms": 0.125, "sort_ms": 0.04,
+          "raster_ms": 0.6}
+    text = gs.format_stats(3_000_000, st, 812.34)
+    assert text.splitlines() == ["FPS: 812.3", "Gaussians: 3000000", "Total: 1.23ms", "SH: 0.00ms",
+                                 "Project: 0.25ms", "Build: 0.12ms", "Sort: 0.04ms", "Raster: 0.60ms"]
+
+
+def test_overlay_font(gs):
+    assert gs.font_glyph(" ") == [0] * 7
+    assert gs.font_glyph("\x7f") == [0] * 7
+    one = gs.font_glyph("1")
+    assert len(one) == 7 and all(r < 32 for r in one) and sum(bin(r).count("1") for r in one) > 5
+    # every character the overlay prints has a glyph
+    for c in "FPS:.0123456789GaussinTotalHProjectBuildSortRasterm":
+        assert any(gs.font_glyph(c)), c

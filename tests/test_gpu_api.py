@@ -110,3 +110,37 @@ def test_server_budget_and_errors(gs):
     srv.wait(srv.submit(sid, cam, out))
     assert out.any()
     srv.close()
+
+
+def test_perf_overlay_draws_the_stats_text(gs):
+    """gs_draw_stats writes exactly the glyph pixels of the formatted lines
+    (white, upright from the displayed top-left corner, row 0 = bottom) and
+    leaves every other pixel of the rendered frame as it was."""
+    torch = pytest.importorskip("torch")
+    ctx = gs.Context(0)
+    sc = gs.scenes.uniform_scene(20_000, seed=12)
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], gs.scenes.grouped_sh(sc["sh"]), 3)
+    W, H = 320, 200
+    cam = gs.look_at((0.2, 0.1, 3.0), (0, 0, 0), (0, 1, 0), 60.0, W, H, 0.1, 100.0)
+    out = torch.zeros((H, W, 4), dtype=torch.uint8, device="cuda")
+    st = gs.render(ctx, scene, cam, gs.RenderConfig(), out)
+    before = out.cpu().numpy().copy()
+    gs.draw_stats(out, W, H, 20_000, st, 123.4)
+    torch.cuda.synchronize()
+    after = out.cpu().numpy()
+    # expected text mask from the formatted lines and the library's font
+    mask = np.zeros((H, W), bool)
+    for ln, text in enumerate(gs.format_stats(20_000, st, 123.4).splitlines()):
+        for col, ch in enumerate(text):
+            rows = gs.font_glyph(ch)
+            for gy in range(7):
+                for gx in range(5):
+                    if (rows[gy] >> (4 - gx)) & 1:
+                        x, y_top = 5 + 6 * col + gx, 5 + 9 * ln + gy
+                        if x < W and y_top < H:
+                            mask[H - 1 - y_top, x] = True
+    assert mask.sum() > 200
+    assert (after[mask] == 255).all()
+    assert np.array_equal(after[~mask], before[~mask])
+    scene.close()
+    ctx.close()
