@@ -389,8 +389,9 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     rc = ensure_sort_scratch(ctx, K);
     if (rc) return rc;
     GS_CUDA(cudaEventRecord(ctx->ev[2], st));
-    EmitArgs ea;
+    EmitArgs ea{};
     ea.n = n;
+    ea.fast = cfg.termination == GS_TERM_TMIN;  // the frame kernel's arithmetic
     ea.num_views = num_views;
     ea.views = ctx->views.as<ViewParams>();
     ea.offsets = ctx->offsets.as<int32_t>();
@@ -604,6 +605,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     BucketEmitArgs ea{};
     ea.n = p.n;
     ea.aggregate = p.tiles_total <= kAggregateMaxTiles;
+    ea.fast = cfg.termination == GS_TERM_TMIN;  // the frame kernel's arithmetic
     ea.slot_count = &dc->slots;
     ea.max_slots = p.items;
     ea.views = ctx->views.as<ViewParams>();
@@ -1320,7 +1322,7 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     *out_num_keys = K;
     if (K > capacity) return fail(GS_ERR_CAPACITY, "tile list capacity exceeded");
     if (K > 0 && (!d_keys || !d_values)) return fail(GS_ERR_INVALID, "null key buffers");
-    EmitArgs ea;
+    EmitArgs ea{};  // exact candidate tests (the stage API's projection is exact)
     ea.n = n;
     ea.num_views = 1;
     ea.views = ctx->views.as<ViewParams>();

@@ -327,7 +327,8 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
             if (c < total) {
                 int tile = 0;
                 const ViewParams& v = a.views[oview];
-                hit = candidate_hit(oe, orr, c - oexcl, v, tile);
+                hit = a.fast ? candidate_hit<true>(oe, orr, c - oexcl, v, tile)
+                             : candidate_hit<false>(oe, orr, c - oexcl, v, tile);
                 gt = v.tile_offset + tile;
             }
             put_keys(a, hit, gt, od, base + (threadIdx.x & ~31) + o);

@@ -356,25 +356,37 @@ struct Ell {
     float cx, cy, cs, sn, ex, ey;
 };
 
-__device__ __forceinline__ void to_ellipse(const Ell& e, const float px, const float py, float& ox, float& oy)
+// FAST (T_min frames): the divisions by the extents and by the edge length
+// become multiplications by hardware reciprocals; the tests are the same.
+template <bool FAST>
+__device__ __forceinline__ void to_ellipse(const Ell& e, const float px, const float py, float& ox, float& oy,
+                                           const float iex, const float iey)
 {
     const float dx = px - e.cx, dy = py - e.cy;
-    ox = (dx * e.cs + dy * e.sn) / e.ex;
-    oy = (dy * e.cs - dx * e.sn) / e.ey;
+    if constexpr (FAST) {
+        ox = (dx * e.cs + dy * e.sn) * iex;
+        oy = (dy * e.cs - dx * e.sn) * iey;
+    } else {
+        ox = (dx * e.cs + dy * e.sn) / e.ex;
+        oy = (dy * e.cs - dx * e.sn) / e.ey;
+    }
 }
 
 __device__ __forceinline__ float len2(const float x, const float y) { return x * x + y * y; }
 
+template <bool FAST>
 __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0y, const float v1x, const float v1y)
 {
     const float dx = v1x - v0x, dy = v1y - v0y;
     const float l2 = dx * dx + dy * dy;
-    const float t = __saturatef(((-v0x) * dx + (-v0y) * dy) / l2);
+    const float num = (-v0x) * dx + (-v0y) * dy;
+    const float t = __saturatef(FAST ? num * rcp_approx(l2) : num / l2);
     const float prx = v0x + t * (v1x - v0x);
     const float pry = v0y + t * (v1y - v0y);
     return len2(prx, pry) < 1.0f;
 }
 
+template <bool FAST = false>
 __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x0, const float y0, const float x1,
                                                      const float y1)
 {
@@ -382,21 +394,22 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
     // The reference ORs all five tests, so a centre strictly inside the tile
     // decides the result; skipping the rest changes nothing.
     if (ov) return true;
+    const float iex = FAST ? rcp_approx(e.ex) : 0.0f, iey = FAST ? rcp_approx(e.ey) : 0.0f;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
     const float rcy = y0 + (y1 - y0) * 0.5f;
     float ux, uy;
-    to_ellipse(e, rcx, rcy, ux, uy);
+    to_ellipse<FAST>(e, rcx, rcy, ux, uy, iex, iey);
     ov |= len2(ux, uy) < 1.0f;
     float p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y;
-    to_ellipse(e, x0, y0, p0x, p0y);
-    to_ellipse(e, x1, y0, p1x, p1y);
-    to_ellipse(e, x1, y1, p2x, p2y);
-    to_ellipse(e, x0, y1, p3x, p3y);
-    ov |= hits_unit_circle(p0x, p0y, p1x, p1y);
-    ov |= hits_unit_circle(p1x, p1y, p2x, p2y);
-    ov |= hits_unit_circle(p2x, p2y, p3x, p3y);
-    ov |= hits_unit_circle(p3x, p3y, p0x, p0y);
+    to_ellipse<FAST>(e, x0, y0, p0x, p0y, iex, iey);
+    to_ellipse<FAST>(e, x1, y0, p1x, p1y, iex, iey);
+    to_ellipse<FAST>(e, x1, y1, p2x, p2y, iex, iey);
+    to_ellipse<FAST>(e, x0, y1, p3x, p3y, iex, iey);
+    ov |= hits_unit_circle<FAST>(p0x, p0y, p1x, p1y);
+    ov |= hits_unit_circle<FAST>(p1x, p1y, p2x, p2y);
+    ov |= hits_unit_circle<FAST>(p2x, p2y, p3x, p3y);
+    ov |= hits_unit_circle<FAST>(p3x, p3y, p0x, p0y);
     return ov;
 }
 
@@ -452,6 +465,7 @@ __device__ __forceinline__ int rect_candidates(const int4 r) { return imax(0, r.
 
 // Candidate c of a tile rectangle, row-major (gaussian_render.cu:466-483).
 // Returns true on overlap and the view-local tile index.
+template <bool FAST = false>
 __device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const int c, const ViewParams& v, int& tile)
 {
     const int lx = c % r.z, ly = c / r.z;
@@ -460,7 +474,7 @@ __device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const 
     const float ty0 = (float)gy * v.tclip_y - 1.0f;
     const float tx1 = tx0 + v.tclip_x;
     const float ty1 = ty0 + v.tclip_y;
-    if (!ellipse_rect_overlap(e, tx0, ty0, tx1, ty1)) return false;
+    if (!ellipse_rect_overlap<FAST>(e, tx0, ty0, tx1, ty1)) return false;
     // Off-screen candidates only arise from the inverted rectangles of NaN
     // axes; their centre test cannot pass for a visible splat.
     if (gx < 0 || gx >= v.tiles_x || gy < 0 || gy >= v.tiles_y) return false;

@@ -72,6 +72,7 @@ struct BucketEmitArgs {
     uint64_t* keys;
     int64_t capacity;
     int32_t aggregate;               // group same-tile cursor atomics of a warp (frames with few tiles)
+    int32_t fast;                    // re-test candidates as the frame kernel did (T_min frames: FAST)
 };
 
 // Frames of at most this many tiles (all views) group the same-tile atomics
@@ -136,6 +137,7 @@ struct EmitArgs {
     uint64_t* keys;
     int32_t* values;
     int64_t capacity;
+    int32_t fast;  // re-test candidates as the frame kernel did (T_min frames: FAST)
 };
 
 // Raster record of one (view, Gaussian) for GS_TERM_TMIN, written by the

@@ -99,6 +99,7 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
 // and when a frame has few tiles, many atomics on one address serialise.
 // With many tiles the atomics spread out and the grouping costs more than
 // it saves.
+template <bool FAST = false>
 __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
                                                uint32_t& mask, uint32_t* tile_count = nullptr,
                                                const bool aggregate = false)
@@ -125,7 +126,7 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
         const int oexcl = __shfl_sync(kFull, w.excl, o);
         bool hit = false;
         int tile = 0;
-        if (c < w.total) hit = candidate_hit(oe, orr, c - oexcl, v, tile);
+        if (c < w.total) hit = candidate_hit<FAST>(oe, orr, c - oexcl, v, tile);
         const unsigned bal = __ballot_sync(kFull, hit);
 if (tile_count && hit) {
             if (aggregate) {
@@ -278,7 +279,7 @@ __global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(Fr
             }
         }
         uint32_t mask;
-        const int hits = warp_count_hits(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr, a.aggregate != 0);
+        const int hits = warp_count_hits<FAST>(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr, a.aggregate != 0);
         int64_t o_out = o;  // where this item's outputs go
         if (BUCKET) {
             const unsigned bal = __ballot_sync(kFull, hits > 0);
@@ -465,7 +466,9 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
         const int oview = __shfl_sync(kFull, view, o);
         bool hit = false;
         int tile = 0;
-        if (c < w.total) hit = candidate_hit(oe, orr, c - oexcl, a.views[oview], tile);
+        if (c < w.total)
+            hit = a.fast ? candidate_hit<true>(oe, orr, c - oexcl, a.views[oview], tile)
+                         : candidate_hit<false>(oe, orr, c - oexcl, a.views[oview], tile);
         const unsigned bal = __ballot_sync(kFull, hit);
         if (hit) {
             const unsigned omask = lane_range_mask(max(oexcl - base, 0), min(oincl - base, 32));
