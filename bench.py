@@ -461,6 +461,9 @@ def run_ours(args, rank, world, local_rank):
 
 
 def main():
+    # a crash in native code prints the Python stack of every thread to stderr
+    import faulthandler
+    faulthandler.enable(all_threads=True)
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
