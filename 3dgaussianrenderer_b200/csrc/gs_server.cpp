@@ -264,6 +264,10 @@ GS_API void gs_server_default_cfg(gs_server_cfg* cfg)
     cfg->num_workers = 2;
     cfg->batch_target_ms = 8.0;
     gs_default_cfg(&cfg->render);
+    // the batches a server forms rarely repeat (scene, view sizes and output
+    // offsets all vary), so capturing graphs would mostly add capture time
+    // to request latency: plain stream launches
+    cfg->render.graph = 0;
 }
 
 GS_API int gs_server_create(int device, const gs_server_cfg* cfg, gs_server** out)

@@ -245,7 +245,8 @@ typedef struct gs_server_cfg {
     int64_t budget_bytes;     /* scenes + frame buffers must fit (150 GiB default) */
     int32_t max_batch_views;  /* views per batched frame */
     int32_t num_workers;      /* batches in flight */
-    gs_render_cfg render;
+    gs_render_cfg render;     /* frame options (default: gs_default_cfg with graph = 0, the batches
+                                 rarely repeat) */
     double batch_target_ms;   /* a batch stops growing once its estimated time exceeds this (8 ms; 0 = off) */
 } gs_server_cfg;
 typedef struct gs_server_stats {
