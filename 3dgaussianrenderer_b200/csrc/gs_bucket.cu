@@ -237,7 +237,9 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
         int64_t toff = 0;
         int tiles_x = 0;
         if (slot < nslots) {
-            view = (int)((int64_t)__ldg(&a.slot_gi[slot]) / a.n);
+            // view * n + i < 2^31 (checked when the frame is planned): a
+            // 32-bit division
+            view = (int)((uint32_t)__ldg(&a.slot_gi[slot]) / (uint32_t)a.n);
             r = unpack_rect(__ldg(&a.rect[slot]));
             cand = rect_candidates(r);
             depth = depth_bits(__ldg(&a.z[slot]));

@@ -153,8 +153,9 @@ __device__ __forceinline__ void block_rank(const uint64_t (&key)[IPT], const int
 // LSD passes over the 8-bit windows covering `mask`, lowest first; the data
 // lives in registers (p order) and goes through shared memory between
 // passes.  Returns true (registers and sm.k / sm.v in sorted p order) when
-// at least one pass ran.
-template <int NT, int IPT>
+// at least one pass ran.  Without CARRY_V the values stay where they are
+// (the keys carry the slot themselves) and sm.v is not touched.
+template <int NT, int IPT, bool CARRY_V = true>
 __device__ __forceinline__ bool radix_passes(uint64_t (&k)[IPT], int32_t (&v)[IPT], uint64_t mask, const Smem& sm)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -167,14 +168,14 @@ __device__ __forceinline__ bool radix_passes(uint64_t (&k)[IPT], int32_t (&v)[IP
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
             sm.k[pos[i]] = k[i];
-            sm.v[pos[i]] = v[i];
+            if (CARRY_V) sm.v[pos[i]] = v[i];
         }
         __syncthreads();
 #pragma unroll
         for (int i = 0; i < IPT; ++i) {
             const int p = warp * 32 * IPT + i * 32 + lane;
             k[i] = sm.k[p];
-            v[i] = sm.v[p];
+            if (CARRY_V) v[i] = sm.v[p];
         }
         __syncthreads();
         any = true;
@@ -242,7 +243,8 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
         }
     }
     const uint64_t vary = varying_bits<NT>(o, n, sm.red) & 0xFFFFFFFF00000000ull;
-    if (!radix_passes<NT, IPT>(k, v, vary, sm)) {
+    // the keys carry their slots: no values through these passes
+    if (!radix_passes<NT, IPT, false>(k, v, vary, sm)) {
         // one depth for the whole tile: to shared memory as they are
 #pragma unroll
         for (int i = 0; i < IPT; ++i) sm.k[warp * 32 * IPT + i * 32 + lane] = k[i];
@@ -257,6 +259,7 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
         for (int i = 0; i < IPT; ++i) {
             const int p = warp * 32 * IPT + i * 32 + lane;
             if (p < m) {
+                v[i] = (int32_t)(uint32_t)k[i];  // the slot, carried through this sort
                 k[i] = (k[i] & 0xFFFFFFFF00000000ull) | (uint32_t)__ldg(&slot_gi[v[i]]);
                 o |= k[i];
                 n &= k[i];
