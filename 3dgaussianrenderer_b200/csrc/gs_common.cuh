@@ -386,6 +386,14 @@ __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0
     return len2(prx, pry) < 1.0f;
 }
 
+// The five tests evaluated with the hardware reciprocal, each result kept
+// as the value compared with 1.  Returns 1 (overlap) or 0 (none) when every
+// value lies clearly on one side of 1 (more than 1e-3 away; with the tile's
+// corners within 64 ellipse radii the reciprocals move the values by less
+// than 1e-3, so the IEEE evaluation decides the same), -1 otherwise.
+__device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
+                                                          const float x1, const float y1);
+
 template <bool FAST = false>
 __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x0, const float y0, const float x1,
                                                      const float y1)
@@ -394,6 +402,12 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
     // The reference ORs all five tests, so a centre strictly inside the tile
     // decides the result; skipping the rest changes nothing.
     if (ov) return true;
+    if constexpr (!FAST) {
+        // the approximate evaluation decides whenever it is clear of the
+        // threshold; only near-boundary cases run the IEEE divisions
+        const int clear = ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
+        if (clear >= 0) return clear != 0;
+    }
     const float iex = FAST ? rcp_approx(e.ex) : 0.0f, iey = FAST ? rcp_approx(e.ey) : 0.0f;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
@@ -411,6 +425,45 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
     ov |= hits_unit_circle<FAST>(p2x, p2y, p3x, p3y);
     ov |= hits_unit_circle<FAST>(p3x, p3y, p0x, p0y);
     return ov;
+}
+
+__device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
+                                                          const float x1, const float y1)
+{
+    constexpr float kMargin = 1e-3f;
+    const float iex = rcp_approx(e.ex), iey = rcp_approx(e.ey);
+    bool unclear = false;
+    auto test = [&](const float v) {  // v < 1 with its margin
+        if (v < 1.0f - kMargin) return true;
+        if (!(v > 1.0f + kMargin)) unclear = true;  // also NaN
+        return false;
+    };
+    const float rcx = x0 + (x1 - x0) * 0.5f;
+    const float rcy = y0 + (y1 - y0) * 0.5f;
+    float ux, uy;
+    to_ellipse<true>(e, rcx, rcy, ux, uy, iex, iey);
+    if (test(len2(ux, uy))) return 1;
+    float px[4], py[4];
+    to_ellipse<true>(e, x0, y0, px[0], py[0], iex, iey);
+    to_ellipse<true>(e, x1, y0, px[1], py[1], iex, iey);
+    to_ellipse<true>(e, x1, y1, px[2], py[2], iex, iey);
+    to_ellipse<true>(e, x0, y1, px[3], py[3], iex, iey);
+    // far corners (an edge 64 ellipse radii away) make the rounding of the
+    // corners matter more than the margin allows: let IEEE decide
+    const float far = fmaxf(fmaxf(fmaxf(fabsf(px[0]), fabsf(py[0])), fmaxf(fabsf(px[1]), fabsf(py[1]))),
+                            fmaxf(fmaxf(fabsf(px[2]), fabsf(py[2])), fmaxf(fabsf(px[3]), fabsf(py[3]))));
+    if (!(far <= 64.0f)) return -1;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int j = (k + 1) & 3;
+        const float dx = px[j] - px[k], dy = py[j] - py[k];
+        const float l2 = dx * dx + dy * dy;
+        const float t = __saturatef(((-px[k]) * dx + (-py[k]) * dy) * rcp_approx(l2));
+        const float prx = px[k] + t * (px[j] - px[k]);
+        const float pry = py[k] + t * (py[j] - py[k]);
+        if (test(len2(prx, pry))) return 1;
+    }
+    return unclear ? -1 : 0;
 }
 
 struct RectF {
