@@ -32,6 +32,11 @@ sys.path.insert(0, ROOT)
 
 VIEWS = 64
 N_GAUSS = 3_000_000
+# DRAM bytes (read + written) of the T_min raster launch of view 0 (1280x720)
+# rendered alone: ncu capture of the second frame of `bench.py --views 1
+# --steps 1 --warmup 1 --no-cpu --no-e2e --no-plain --no-serve` (126.8 MB
+# read, 8.3 MB written; the raster roofline's traffic)
+RASTER_VIEW0_TRAFFIC = 135.1e6
 RING_RADIUS = 15.0
 WORKLOAD = "3M Gaussians SH3, 64-view orbit ring r=15, 1280x720/1600x900/1920x1080 cycling, one batched frame"
 
@@ -398,35 +403,33 @@ def run_ours(args, rank, world, local_rank):
     hbm, peak_kind = peaks()
     per = {k: v / args.steps for k, v in stages.items()}
     K = keys
-    # Algorithmic bytes per launch of the HBM-bound stages, per view as the
-    # scope table states them: SH + projection N (32 + 12 (d + 1)^2 + 48),
-    # build N 52 + 12 K.  (The frame kernel reads the scene once per 16
-    # views, so its DRAM traffic is well below its algorithmic bytes.)
-    n_items = N_GAUSS * VIEWS
-    alg = {
-        "project_ms": n_items * (32 + 12 * 16 + 48),
-        "build_tile_ms": n_items * 52 + K * 12,
-    }
-    ach = {k: alg[k] / (per[k] / 1e3) / 1e9 for k in alg if per[k] > 0}
-    dom = max(per, key=per.get)
-    # DRAM bytes of one 64-view launch of the frame kernel: an ncu capture
-    # of a 4-view frame (672.7 MB read, 509.2 MB written; the scene is read
-    # once per 16 views, the writes grow with the views), scaled to 64 views
+    # Frame kernel against HBM.  Algorithmic bytes of one launch: the scene
+    # (32 B position + scale/rotation, 12 (d + 1)^2 = 192 B SH per Gaussian)
+    # read once per block of 16 views, and the 48-byte splat record per
+    # (view, Gaussian) of the scope table written: ceil(V / 16) N 224 + V N 48.
+    # traffic: DRAM bytes of an ncu capture of a 4-view frame (672.7 MB read,
+    # 509.2 MB written), scaled to 64 views (reads per 16 views, writes per
+    # view).  The kernel is issue-bound, far under this roof.
+    alg_frame = ((VIEWS + 15) // 16) * N_GAUSS * (32 + 12 * 16) + VIEWS * N_GAUSS * 48
     frame_traffic = 672.7e6 * ((VIEWS + 15) // 16) + 509.2e6 / 4 * VIEWS if VIEWS == 64 else None
-    roof = {"bound": "hbm", "kernel": "frame_project (SH + projection + tile counts)",
-            "achieved": ach["project_ms"], "peak": hbm, "unit": "GB/s", "frac": ach["project_ms"] / hbm,
-            "traffic": frame_traffic,
-            "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind,
-            "stage_ms": per, "stage_gbs": ach, "dominant_stage": dom,
-            "dominant_bound": "fp32 + MUFU (raster blends; sort of small tiles fused in)"}
+    frame_gbs = alg_frame / (per["project_ms"] / 1e3) / 1e9 if per["project_ms"] > 0 else None
+    frame_roof = {"bound": "hbm", "kernel": "frame_project (SH + projection + tile counts)",
+                  "achieved": frame_gbs, "peak": hbm, "unit": "GB/s",
+                  "frac": frame_gbs / hbm if frame_gbs else None, "traffic": frame_traffic,
+                  "algorithmic_bytes": alg_frame,
+                  "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
+    dom = max(per, key=per.get)
     cpu = cpu_baseline(gs, sc, cams, sample_views=1) if (world == 1 and not args.no_cpu) else None
-    # Raster roofline (FP32 pipe) of view 0 rendered alone: work = 11 FP32
-    # lane operations per (pixel, entry) evaluation of the record raster (the
-    # packed blend: exponent 2 fma + column terms, w, 3 colour fma, T update,
-    # saturation), the evaluations the GPU's warp-culled raster executes as
-    # counted by the oracle; time = the raster stage; peak = 148 SMs x 128
-    # FP32 lanes x the SM clock sampled during the timed region.  The oracle's
-    # count without culling (every entry until T < t_min) is given beside it.
+    # The dominant kernel, the T_min raster, against the FP32 pipe (it is
+    # neither HBM- nor tensor-bound), for view 0 rendered alone: work = 11
+    # FP32 lane operations per (pixel, entry) evaluation of the packed blend
+    # (exponent: 2 fma + the column terms; w; 3 colour fma; T update), the
+    # evaluations the GPU's warp-culled walk executes as counted by the
+    # oracle's model of it; time = the raster stage; peak = 148 SMs x 128
+    # FP32 lanes x the SM clock sampled during the timed region (nominal:
+    # there is no measured FP32 peak).  The oracle's count without the cull
+    # (every entry until T < t_min) is given beside it.  traffic: DRAM bytes
+    # of an ncu capture of the same single-view launch.
     raster_roof = None
     if cpu and cpu.get("block_evals_view0") and raster_view0_ms:
         clk_mhz = (clocks or {}).get("sm_mhz") or 1965.0
@@ -434,10 +437,13 @@ def run_ours(args, rank, world, local_rank):
         ach = 11.0 * cpu["block_evals_view0"] / (raster_view0_ms / 1e3) / 1e9
         raster_roof = {"bound": "fp32", "kernel": "raster_rec (T_min records, per-tile sort fused)",
                        "achieved": ach, "peak": peak_gops, "unit": "Gop/s", "frac": ach / peak_gops,
+                       "traffic": RASTER_VIEW0_TRAFFIC,
                        "evals_executed": cpu["block_evals_view0"], "evals_unculled": cpu["evals_view0"],
                        "ops_per_eval": 11, "raster_ms": raster_view0_ms,
                        "view": f"view 0 ({cams[0].GetWidth()}x{cams[0].GetHeight()}) rendered alone",
                        "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x sampled SM clock"}
+    roof = raster_roof or frame_roof
+    roof = dict(roof, stage_ms=per, dominant_stage=dom)
     line = {
         "metric": "views/s", "value": value, "unit": "views/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -452,7 +458,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_ref_mode_1024": ref1024,
         "served": served,
         "roofline": roof,
-        "raster_roofline": raster_roof,
+        "frame_roofline": frame_roof,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
