@@ -215,10 +215,10 @@ __device__ __forceinline__ int64_t acquire_tile(unsigned long long* counter)
 // BUCKET: no scan at all -- each overlapping (view, Gaussian) takes a slot
 // (one atomic per warp) and adds its overlaps to the per-tile counts; the
 // blocks are independent and run in launch order.
-// Blocks per SM: SH degree 3 keeps 80 registers (3 blocks); lower degrees
-// run faster at 4 blocks (64 registers)
+// Blocks per SM: 4 (64 registers); the exact projection at SH degree 3
+// keeps 80 registers (3 blocks)
 template <int DEG, bool BUCKET, bool FAST>
-__global__ void __launch_bounds__(256, DEG >= 3 ? 3 : 4) frame_project_kernel(FrameArgs a)
+__global__ void __launch_bounds__(256, (DEG >= 3 && !FAST) ? 3 : 4) frame_project_kernel(FrameArgs a)
 {
     extern __shared__ __align__(128) float s_sh[];  // [3*(DEG+1)^2][256]
     __shared__ __align__(8) uint64_t s_bar;
