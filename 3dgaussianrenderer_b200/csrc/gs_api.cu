@@ -111,11 +111,24 @@ struct FrameGraph {
     uint64_t last_use = 0;
     int seen = 0;                    // calls with this key
     int failed = 0;                  // capture failed: run this key without a graph
+    int raster_groups = 0;           // raster launched per view group (host-output batches)
 };
 constexpr size_t kMaxGraphs = 8;
 // gs_render_batch_host renders batches of more than this many views in
-// chunks, reading each chunk back while the next one renders.
+// groups, reading each group back while the next one renders.
 constexpr int kHostChunkViews = 16;
+constexpr int kMaxRasterGroups = 8;
+
+// Host read-back overlapped with the frame (T_min bucket frames): the
+// raster runs one view group after the other, each group's end is marked by
+// an event, and the group's images are copied on `copy` after it.
+struct HostCopy {
+    uint8_t* h_rgba = nullptr;
+    cudaStream_t copy = nullptr;
+    int groups = 0;
+    int first_view[kMaxRasterGroups + 1] = {};  // group g = views [first_view[g], first_view[g + 1])
+    size_t first_byte[kMaxRasterGroups + 1] = {};
+};
 
 std::atomic<uint64_t> g_scene_uid{1};
 
@@ -157,6 +170,7 @@ struct gs_ctx {
     int64_t per_view_capacity = 0;         // Gaussians * views the splat buffers hold
     cudaStream_t cap_stream = nullptr;     // graph capture
     cudaStream_t copy_stream = nullptr;    // image read-back of the host-output batches
+    cudaEvent_t ev_group[kMaxRasterGroups] = {};  // end of each raster view group
     bool tile_count_dirty = true;          // tile counts may be nonzero: clear before the next frame
     std::vector<FrameGraph> graphs;
     uint64_t use_clock = 0;
@@ -476,6 +490,7 @@ struct FramePlan {
     int num_views = 0;
     int64_t n = 0, groups = 0, blocks = 0, items = 0, tiles_total = 0;
     int vpb = 0, deg = 0;
+    const HostCopy* host_copy = nullptr;  // non-null: raster per view group, each group's end marked
 };
 
 // Validates the frame, fills the pinned view parameters and makes the
@@ -652,7 +667,24 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ra.slot_gi = ctx->offsets.as<int32_t>();
     ra.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     ra.order = ctx->tile_order.as<int32_t>();
-    launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, p.num_views > 1, ctx->num_sms, st);
+    if (p.host_copy && p.host_copy->groups > 1 && ra.rec) {
+        // one launch per view group, in view order; a group's images are
+        // complete at its event
+        const HostCopy& hc = *p.host_copy;
+        ra.order = nullptr;
+        for (int g = 0; g < hc.groups; ++g) {
+            const int v0 = hc.first_view[g], v1 = hc.first_view[g + 1];
+            const int64_t t0 = ctx->h_views[v0].tile_offset;
+            const int64_t t1 = v1 < p.num_views ? ctx->h_views[v1].tile_offset : p.tiles_total;
+            RasterArgs rg = ra;
+            rg.tile_base = t0;
+            rg.num_tiles_total = t1 - t0;
+            launch_raster(rg, cfg.tile_w, cfg.tile_h, cfg.termination, false, ctx->num_sms, st);
+            GS_CUDA(record(ctx->ev_group[g], st, capturing));
+        }
+    } else {
+        launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, p.num_views > 1, ctx->num_sms, st);
+    }
     GS_CUDA(cudaGetLastError());
     GS_CUDA(record(ctx->ev[5], st, capturing));
     GS_CUDA(cudaMemcpyAsync(ctx->h_counters, dc, sizeof(Counters), cudaMemcpyDeviceToHost, st));
@@ -725,11 +757,13 @@ bool capture_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg& cfg,
 // With cfg.graph, the second frame with the same scene, options, view sizes
 // and outputs is captured into a CUDA graph and later ones replay it.
 int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
-                     uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
+                     uint8_t* const* outs, gs_stats* stats, cudaStream_t st, const HostCopy* hc = nullptr)
 {
     FramePlan p;
     int rc = plan_bucket_frame(ctx, scene, cams, num_views, cfg, outs, p);
     if (rc) return rc;
+    p.host_copy = hc;
+    const int raster_groups = hc ? hc->groups : 0;
     if (!ctx->keys0.p) {
         rc = ensure_key_buffers(ctx, std::max<int64_t>(p.items, 1 << 20));
         if (rc) return rc;
@@ -739,7 +773,7 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
     FrameGraph* g = nullptr;
     if (cfg.graph) {
         for (FrameGraph& x : ctx->graphs)
-            if (same_frame(x, scene, cfg, cams, num_views, outs)) g = &x;
+            if (same_frame(x, scene, cfg, cams, num_views, outs) && x.raster_groups == raster_groups) g = &x;
         if (!g) {
             if (ctx->graphs.size() >= kMaxGraphs) {
                 auto lru = std::min_element(ctx->graphs.begin(), ctx->graphs.end(),
@@ -751,6 +785,7 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
             g = &ctx->graphs.back();
             g->scene_uid = scene->uid;
             g->cfg = cfg;
+            g->raster_groups = raster_groups;
             g->outs.assign(outs, outs + num_views);
             g->sizes.resize(2 * (size_t)num_views);
             for (int v = 0; v < num_views; ++v) {
@@ -780,6 +815,16 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
             rc = enqueue_bucket_frame(ctx, scene, cfg, p, st, false);
             if (rc) return rc;
             replayed = false;
+        }
+        if (hc && hc->groups > 1 && cfg.termination == GS_TERM_TMIN) {
+            // each group's images go to the host once its raster is done,
+            // while the next group renders (a redone frame copies again)
+            for (int gi = 0; gi < hc->groups; ++gi) {
+                GS_CUDA(cudaStreamWaitEvent(hc->copy, ctx->ev_group[gi], 0));
+                const size_t b0 = hc->first_byte[gi], b1 = hc->first_byte[gi + 1];
+                GS_CUDA(cudaMemcpyAsync(hc->h_rgba + b0, outs[hc->first_view[gi]], b1 - b0, cudaMemcpyDeviceToHost,
+                                        hc->copy));
+            }
         }
         const cudaError_t se = cudaStreamSynchronize(st);
         if (se != cudaSuccess) {
@@ -933,6 +978,7 @@ int gs_ctx_create(int device, gs_ctx** out)
     std::memset(c->h_init, 0, sizeof(Counters));
     std::memset(c->h_counters, 0, sizeof(Counters));
     for (auto& ev : c->ev) cudaEventCreate(&ev);
+    for (auto& ev : c->ev_group) cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
     *out = c;
     return GS_OK;
 }
@@ -955,6 +1001,8 @@ int gs_ctx_destroy(gs_ctx* ctx)
     if (ctx->h_init) cudaFreeHost(ctx->h_init);
     if (ctx->h_views) cudaFreeHost(ctx->h_views);
     for (auto& ev : ctx->ev)
+        if (ev) cudaEventDestroy(ev);
+    for (auto& ev : ctx->ev_group)
         if (ev) cudaEventDestroy(ev);
     delete ctx;
     return GS_OK;
@@ -1194,12 +1242,30 @@ int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* ca
         GS_CUDA(cudaStreamSynchronize(st));
         return GS_OK;
     }
-    // Larger batches render in chunks of kHostChunkViews views; each chunk's
+    if (!ctx->copy_stream) GS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
+    if (cfg->ordering == GS_ORDER_BUCKETS && cfg->termination == GS_TERM_TMIN) {
+        // one frame for all views; its raster runs in view groups, each
+        // group read back on the copy stream while the next one renders
+        HostCopy hc;
+        hc.h_rgba = h_rgba;
+        hc.copy = ctx->copy_stream;
+        hc.groups = std::min(kMaxRasterGroups, (num_views + kHostChunkViews - 1) / kHostChunkViews);
+        const int per = (num_views + hc.groups - 1) / hc.groups;
+        for (int g = 0; g <= hc.groups; ++g) {
+            hc.first_view[g] = std::min(num_views, g * per);
+            hc.first_byte[g] = hc.first_view[g] < num_views ? offs[hc.first_view[g]] : total;
+        }
+        const int rc = run_frame_bucket(ctx, scene, cams, num_views, *cfg, outs.data(), stats, st, &hc);
+        const cudaError_t se = cudaStreamSynchronize(ctx->copy_stream);
+        if (rc) return rc;
+        if (se != cudaSuccess) return cuda_fail(se, "image copy");
+        return GS_OK;
+    }
+    // Other frames render in chunks of kHostChunkViews views; each chunk's
     // images are copied to the host on a second stream while the next chunk
     // renders (a frame returns with its stream synchronised, so the chunk is
     // complete when its copy is queued).  The frame kernel reads the scene
     // once per 16 views anyway, so the chunks cost little batching.
-    if (!ctx->copy_stream) GS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
     gs_stats acc{};
     acc.graph_replay = 1;
     int rc = GS_OK;

@@ -174,7 +174,8 @@ struct RasterArgs {
     const ViewParams* views;          // persistent kernel: all views
     int32_t num_views;
     int32_t write_empty;              // 1: tiles without entries are written as (0,0,0,0)
-    int64_t num_tiles_total;          // sum of the views' tiles
+    int64_t num_tiles_total;          // sum of the views' tiles (of this launch's tiles when tile_base is used)
+    int64_t tile_base;                // record raster without `order`: CTA b draws global tile tile_base + b
     const int32_t* ranges;            // [2 * num_tiles_total]
     const int32_t* values;
     const float2* xy;                 // indexed by value (reference-mode kernel)

@@ -491,7 +491,7 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
     __shared__ f2 s_bl[NW][32];
     __shared__ FusedSortSmem<TW * TH / 2> fs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : (int64_t)blockIdx.x;
+    const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : a.tile_base + (int64_t)blockIdx.x;
     int vi = 0;
     if (a.num_views > 1) {
         int hi = a.num_views - 1;

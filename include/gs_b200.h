@@ -158,10 +158,11 @@ GS_API int gs_render_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* c
 GS_API int gs_render_batch(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
                     const gs_render_cfg* cfg, uint8_t* const* d_rgba, gs_stats* stats, void* stream);
 /* Same, images copied into one host buffer: view v at byte offset
- * sum_{u<v} 4*W_u*H_u.  Batches of more than 16 views are rendered 16 views
- * at a time, each group read back (on a second stream) while the next one
- * renders; the stats then add up the groups.  Returns when every image is
- * in h_rgba. */
+ * sum_{u<v} 4*W_u*H_u.  Batches of more than 16 views are read back in
+ * groups of views while the next group renders: T_min bucket frames render
+ * all views in one frame whose raster runs group by group; other frames
+ * render 16 views at a time (the stats then add up the frames).  Returns
+ * when every image is in h_rgba. */
 GS_API int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
                          const gs_render_cfg* cfg, uint8_t* h_rgba, gs_stats* stats, void* stream);
 
