@@ -117,6 +117,7 @@ constexpr size_t kMaxGraphs = 8;
 // gs_render_batch_host renders batches of more than this many views in
 // groups, reading each group back while the next one renders.
 constexpr int kHostChunkViews = 16;
+constexpr int kHostGroupViews = 8;  // views per raster group of a T_min host batch
 constexpr int kMaxRasterGroups = 8;
 
 // Host read-back overlapped with the frame (T_min bucket frames): the
@@ -1249,7 +1250,7 @@ int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* ca
         HostCopy hc;
         hc.h_rgba = h_rgba;
         hc.copy = ctx->copy_stream;
-        hc.groups = std::min(kMaxRasterGroups, (num_views + kHostChunkViews - 1) / kHostChunkViews);
+        hc.groups = std::min(kMaxRasterGroups, (num_views + kHostGroupViews - 1) / kHostGroupViews);
         const int per = (num_views + hc.groups - 1) / hc.groups;
         for (int g = 0; g <= hc.groups; ++g) {
             hc.first_view[g] = std::min(num_views, g * per);
