@@ -346,7 +346,7 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
         const int idx2 = (loader && n2 < count) ? slot_at(a, sk, first, n2) : 0;
         const int j0 = 32 * buf;
         if (nb == 32) {
-#pragma unroll 4
+#pragma unroll 8
             for (int j = j0; j < j0 + 32; ++j) blend_ref_pair(cx, cyy, sm, j, R, G, B, TT);
         } else {
             for (int j = j0; j < j0 + nb; ++j) blend_ref_pair(cx, cyy, sm, j, R, G, B, TT);
