@@ -34,9 +34,9 @@ VIEWS = 64
 N_GAUSS = 3_000_000
 # DRAM bytes (read + written) of the T_min raster launch of view 0 (1280x720)
 # rendered alone: ncu capture of the second frame of `bench.py --views 1
-# --steps 1 --warmup 1 --no-cpu --no-e2e --no-plain --no-serve` (126.8 MB
-# read, 8.3 MB written; the raster roofline's traffic)
-RASTER_VIEW0_TRAFFIC = 135.1e6
+# --steps 1 --warmup 1 --no-cpu --no-e2e --no-plain --no-serve` (128.2 MB
+# read, 7.0 MB written; the raster roofline's traffic)
+RASTER_VIEW0_TRAFFIC = 135.2e6
 RING_RADIUS = 15.0
 WORKLOAD = "3M Gaussians SH3, 64-view orbit ring r=15, 1280x720/1600x900/1920x1080 cycling, one batched frame"
 
