@@ -96,6 +96,10 @@ class gs_stats(ctypes.Structure):
         return {name: getattr(self, name) for name, _ in self._fields_}
 
 
+class gs_tune_result(ctypes.Structure):
+    _fields_ = [("cfg", gs_render_cfg), ("ms", ctypes.c_double)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I32 = ctypes.c_int32
@@ -135,6 +139,11 @@ _sig("gs_render_batch", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POIN
      ctypes.POINTER(_P), ctypes.POINTER(gs_stats), _P)
 _sig("gs_render_batch_host", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(gs_render_cfg), _P,
      ctypes.POINTER(gs_stats), _P)
+_sig("gs_autotune", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(gs_render_cfg), _I32,
+     ctypes.POINTER(gs_render_cfg), ctypes.POINTER(ctypes.c_double), ctypes.POINTER(gs_tune_result), _I32,
+     ctypes.POINTER(_I32), _P)
+_sig("gs_autotune_lookup", _I, _P, _I64, _I32, _I32, _I32, ctypes.POINTER(gs_render_cfg), ctypes.POINTER(_I32))
+_sig("gs_autotune_entries", _I32, _P)
 _sig("gs_stage_sh", _I, _I64, _P, _P, _I32, _I32, ctypes.POINTER(gs_camera), _P, _P)
 _sig("gs_stage_project", _I, _I64, _P, _P, ctypes.POINTER(gs_camera), _P, _P, _P, _P, _P)
 _sig("gs_stage_build", _I, _P, _I64, _P, _P, _P, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P, _P,
@@ -389,6 +398,37 @@ def render_batch_host(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig,
     check(lib.gs_render_batch_host(ctx.h, scene.h, arr, len(cams), ctypes.byref(c), _ptr(out), ctypes.byref(st),
                                    _stream_ptr(stream)), "gs_render_batch_host")
     return st.as_dict()
+
+
+def _from_c(c: gs_render_cfg) -> "RenderConfig":
+    return RenderConfig(c.sh_max_degree, c.termination, c.t_min, c.tile_w, c.tile_h, c.ordering, c.sort_variant,
+                        c.views_per_block, c.graph)
+
+
+def autotune(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig, iterations: int = 5, stream=None):
+    """Times the batching knobs (tile shape, views per block, onesweep tile
+    shape) on this batch and stores the fastest in the context's table for
+    the batch's (N, resolution, views) bucket.  Returns (best RenderConfig,
+    its ms per batch, [(RenderConfig, ms) of every timed candidate])."""
+    arr = (gs_camera * len(cams))(*[c.c for c in cams])
+    c = cfg.c()
+    best = gs_render_cfg()
+    best_ms = ctypes.c_double()
+    res = (gs_tune_result * 64)()
+    count = _I32()
+    check(lib.gs_autotune(ctx.h, scene.h, arr, len(cams), ctypes.byref(c), iterations, ctypes.byref(best),
+                          ctypes.byref(best_ms), res, 64, ctypes.byref(count), _stream_ptr(stream)), "gs_autotune")
+    return _from_c(best), best_ms.value, [(_from_c(r.cfg), r.ms) for r in res[:min(count.value, 64)]]
+
+
+def autotune_lookup(ctx: Context, n: int, width: int, height: int, num_views: int, cfg: RenderConfig):
+    """The tuned knobs of the bucket applied to cfg, or None when the bucket
+    was not tuned."""
+    c = cfg.c()
+    found = _I32()
+    check(lib.gs_autotune_lookup(ctx.h, n, width, height, num_views, ctypes.byref(c), ctypes.byref(found)),
+          "gs_autotune_lookup")
+    return _from_c(c) if found.value else None
 
 
 # ---------------------------------------------------------------------------

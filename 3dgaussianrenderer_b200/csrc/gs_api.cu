@@ -131,6 +131,17 @@ struct HostCopy {
     size_t first_byte[kMaxRasterGroups + 1] = {};
 };
 
+// A tuned bucket of gs_autotune: the batching knobs that were fastest for
+// scenes of 2^n_log2 .. 2^(n_log2+1) Gaussians, views of 2^px_log2 ..
+// 2^(px_log2+1) pixels and a view count in views_bucket.
+struct TuneEntry {
+    int32_t n_log2 = 0, px_log2 = 0, views_bucket = 0, termination = 0, ordering = 0;
+    int32_t tile_w = 16, tile_h = 16, views_per_block = 0, sort_variant = 0;
+    double ms = 0.0;
+    uint64_t stamp = 0;  // insertion order: the oldest entry goes when the table is full
+};
+constexpr size_t kMaxTuneEntries = 256;
+
 std::atomic<uint64_t> g_scene_uid{1};
 
 }  // namespace
@@ -175,6 +186,8 @@ struct gs_ctx {
     bool tile_count_dirty = true;          // tile counts may be nonzero: clear before the next frame
     std::vector<FrameGraph> graphs;
     uint64_t use_clock = 0;
+    std::vector<TuneEntry> tune;           // gs_autotune's table
+    uint64_t tune_clock = 0;
 };
 
 namespace {
@@ -873,6 +886,78 @@ int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num
     return run_frame_bucket(ctx, scene, cams, num_views, cfg, outs, stats, st);
 }
 
+// floor(log2(x)) for x >= 1, -1 for x <= 0
+int32_t floor_log2(int64_t x)
+{
+    int32_t b = -1;
+    for (; x > 0; x >>= 1) ++b;
+    return b;
+}
+
+int32_t views_bucket(int num_views)
+{
+    return num_views <= 1 ? 0 : num_views <= 4 ? 1 : num_views <= 8 ? 2 : num_views <= 16 ? 3 : num_views <= 32 ? 4 : 5;
+}
+
+TuneEntry tune_key(int64_t n, int64_t pixels, int num_views, const gs_render_cfg& cfg)
+{
+    TuneEntry e;
+    e.n_log2 = floor_log2(n);
+    e.px_log2 = floor_log2(pixels);
+    e.views_bucket = views_bucket(num_views);
+    e.termination = cfg.termination;
+    e.ordering = cfg.ordering;
+    return e;
+}
+
+bool same_bucket(const TuneEntry& a, const TuneEntry& b)
+{
+    return a.n_log2 == b.n_log2 && a.px_log2 == b.px_log2 && a.views_bucket == b.views_bucket &&
+           a.termination == b.termination && a.ordering == b.ordering;
+}
+
+// The knob settings gs_autotune times: tile shapes only where the images do
+// not depend on them (per-pixel termination), views per block only where
+// they change the frame kernel's grouping (distinct min(V, vpb)), onesweep
+// tile shapes only for onesweep frames.
+std::vector<gs_render_cfg> tune_candidates(const gs_render_cfg& base, int num_views)
+{
+    static const int kShapes[3][2] = {{16, 16}, {16, 8}, {8, 8}};
+    std::vector<std::pair<int, int>> shapes;
+    if (base.termination == GS_TERM_TMIN)
+        for (const auto& s : kShapes) shapes.emplace_back(s[0], s[1]);
+    else
+        shapes.emplace_back(base.tile_w, base.tile_h);
+    std::vector<int> vpbs;
+    if (num_views > 8) {
+        int last = 0;
+        for (int v : {8, 16, 32}) {
+            const int eff = std::min(num_views, v);
+            if (eff != last) vpbs.push_back(v);
+            last = eff;
+        }
+    } else {
+        vpbs.push_back(base.views_per_block);
+    }
+    std::vector<int> variants;
+    if (base.ordering == GS_ORDER_ONESWEEP)
+        for (int v = 0; v < kSortVariants; ++v) variants.push_back(v);
+    else
+        variants.push_back(base.sort_variant);
+    std::vector<gs_render_cfg> out;
+    for (const auto& s : shapes)
+        for (int vpb : vpbs)
+            for (int sv : variants) {
+                gs_render_cfg c = base;
+                c.tile_w = s.first;
+                c.tile_h = s.second;
+                c.views_per_block = vpb;
+                c.sort_variant = sv;
+                out.push_back(c);
+            }
+    return out;
+}
+
 }  // namespace
 
 // ============================================================================
@@ -1475,6 +1560,115 @@ int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_
     launch_raster(ra, cfg->tile_w, cfg->tile_h, cfg->termination, false, 148, (cudaStream_t)stream);
     GS_CUDA(cudaGetLastError());
     return GS_OK;
+}
+
+int gs_autotune(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                const gs_render_cfg* base, int32_t iterations, gs_render_cfg* best, double* best_ms,
+                gs_tune_result* results, int32_t results_capacity, int32_t* num_results, void* stream)
+{
+    if (!ctx || !scene || !cams || !base || !best || num_views <= 0) return fail(GS_ERR_INVALID, "null argument");
+    if (iterations < 1 || (results_capacity > 0 && !results)) return fail(GS_ERR_INVALID, "bad tuning arguments");
+    if (!valid_cfg(*base)) return fail(GS_ERR_INVALID, "invalid render cfg");
+    int64_t total = 0, pixels = 0;
+    std::vector<size_t> offs((size_t)num_views);
+    for (int v = 0; v < num_views; ++v) {
+        if (!valid_cam(&cams[v])) return fail(GS_ERR_INVALID, "invalid camera");
+        offs[v] = (size_t)total;
+        total += 4 * (int64_t)cams[v].width * cams[v].height;
+        pixels = std::max<int64_t>(pixels, (int64_t)cams[v].width * cams[v].height);
+    }
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    if (ctx->image.ensure((size_t)total)) return fail(GS_ERR_OOM, "image");
+    std::vector<uint8_t*> outs((size_t)num_views);
+    for (int v = 0; v < num_views; ++v) outs[v] = ctx->image.as<uint8_t>() + offs[v];
+    cudaStream_t st = (cudaStream_t)stream;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    GS_CUDA(cudaEventCreate(&e0));
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return cuda_fail(cudaGetLastError(), "tuning events");
+    }
+
+    const std::vector<gs_render_cfg> cands = tune_candidates(*base, num_views);
+    int rc = GS_OK, timed = 0, win = -1;
+    double win_ms = 0.0;
+    std::vector<float> times((size_t)iterations);
+    for (size_t i = 0; i < cands.size() && rc == GS_OK; ++i) {
+        const gs_render_cfg& c = cands[i];
+        int r = GS_OK;
+        for (int w = 0; w < 2 && r == GS_OK; ++w) r = run_frame(ctx, scene, cams, num_views, c, outs.data(), nullptr, st);
+        for (int it = 0; it < iterations && r == GS_OK; ++it) {
+            cudaEventRecord(e0, st);
+            r = run_frame(ctx, scene, cams, num_views, c, outs.data(), nullptr, st);
+            cudaEventRecord(e1, st);
+            if (r == GS_OK && cudaEventSynchronize(e1) != cudaSuccess) r = cuda_fail(cudaGetLastError(), "tuning");
+            times[it] = ms_between(e0, e1);
+        }
+        if (r == GS_OK) {
+            std::sort(times.begin(), times.end());
+            const double ms = times[(size_t)iterations / 2];
+            if (timed < results_capacity) results[timed] = gs_tune_result{c, ms};
+            ++timed;
+            if (win < 0 || ms < win_ms) win = (int)i, win_ms = ms;
+        } else if (r == GS_ERR_OOM || r == GS_ERR_CAPACITY) {
+            cudaGetLastError();  // this setting does not fit: the others may
+        } else {
+            rc = r;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (num_results) *num_results = timed;
+    if (rc) return rc;
+    if (win < 0) return fail(GS_ERR_OOM, "no knob setting fit in device memory");
+
+    TuneEntry e = tune_key(scene->n, pixels, num_views, *base);
+    e.tile_w = cands[win].tile_w;
+    e.tile_h = cands[win].tile_h;
+    e.views_per_block = cands[win].views_per_block;
+    e.sort_variant = cands[win].sort_variant;
+    e.ms = win_ms;
+    e.stamp = ++ctx->tune_clock;
+    auto it = std::find_if(ctx->tune.begin(), ctx->tune.end(), [&](const TuneEntry& x) { return same_bucket(x, e); });
+    if (it != ctx->tune.end()) {
+        *it = e;
+    } else {
+        if (ctx->tune.size() >= kMaxTuneEntries)
+            ctx->tune.erase(std::min_element(ctx->tune.begin(), ctx->tune.end(),
+                                             [](const TuneEntry& a, const TuneEntry& b) { return a.stamp < b.stamp; }));
+        ctx->tune.push_back(e);
+    }
+    *best = cands[win];
+    if (best_ms) *best_ms = win_ms;
+    return GS_OK;
+}
+
+int gs_autotune_lookup(gs_ctx* ctx, int64_t n, int32_t width, int32_t height, int32_t num_views, gs_render_cfg* cfg,
+                       int32_t* found)
+{
+    if (!ctx || !cfg || !found) return fail(GS_ERR_INVALID, "null argument");
+    if (n < 0 || width <= 0 || height <= 0 || num_views <= 0) return fail(GS_ERR_INVALID, "bad bucket");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    const TuneEntry k = tune_key(n, (int64_t)width * height, num_views, *cfg);
+    *found = 0;
+    for (const TuneEntry& e : ctx->tune)
+        if (same_bucket(e, k)) {
+            cfg->tile_w = e.tile_w;
+            cfg->tile_h = e.tile_h;
+            cfg->views_per_block = e.views_per_block;
+            cfg->sort_variant = e.sort_variant;
+            *found = 1;
+            break;
+        }
+    return GS_OK;
+}
+
+int32_t gs_autotune_entries(gs_ctx* ctx)
+{
+    if (!ctx) return 0;
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    return (int32_t)ctx->tune.size();
 }
 
 int64_t gs_num_tiles(int32_t width, int32_t height, const gs_render_cfg* cfg)

@@ -116,14 +116,14 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(rows)}
 
 
-def cpu_baseline(gs, sc, cams, sample_views=1, threads=None):
-    """The oracle (CPU rendition of the five stages) over a bounded sample of views."""
+def cpu_baseline(gs, sc, cams, rc, sample_views=1, threads=None):
+    """The oracle (CPU rendition of the five stages) over a bounded sample of
+    views, with the render options of the GPU leg."""
     import oracle
     O = oracle.get()
     if threads:
         O.set_threads(threads)
     sh = gs.scenes.grouped_sh(sc["sh"])
-    rc = gs.RenderConfig()
     t0 = time.perf_counter()
     for v in range(sample_views):
         O.render(sc, sh, cams[v], rc)
@@ -307,6 +307,17 @@ def run_ours(args, rank, world, local_rank):
     sh = gs.scenes.grouped_sh(sc["sh"])
     scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
     rc = gs.RenderConfig()
+    tuned = None
+    if not args.no_autotune:
+        # the project's autotuner picks the batching knobs (tile shape, views
+        # per block) for this (N, resolution, views) bucket, outside the
+        # timed region; every rank tunes its own replica
+        best, best_ms, cands = gs.autotune(ctx, scene, cams, rc, iterations=3, stream=stream)
+        rc = best
+        tuned = {"picked": {"tile": f"{best.tile_w}x{best.tile_h}", "views_per_block": best.views_per_block,
+                            "ms": best_ms},
+                 "candidates": [{"tile": f"{c.tile_w}x{c.tile_h}", "views_per_block": c.views_per_block, "ms": m}
+                                for c, m in cands]}
     outs = [torch.empty((c.GetHeight(), c.GetWidth(), 4), dtype=torch.uint8, device=dev) for c in cams]
 
     def step():
@@ -419,7 +430,7 @@ def run_ours(args, rank, world, local_rank):
                   "algorithmic_bytes": alg_frame,
                   "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
     dom = max(per, key=per.get)
-    cpu = cpu_baseline(gs, sc, cams, sample_views=1) if (world == 1 and not args.no_cpu) else None
+    cpu = cpu_baseline(gs, sc, cams, rc, sample_views=1) if (world == 1 and not args.no_cpu) else None
     # The dominant kernel, the T_min raster, against the FP32 pipe (it is
     # neither HBM- nor tensor-bound), for view 0 rendered alone: work = 11
     # FP32 lane operations per (pixel, entry) evaluation of the packed blend
@@ -437,7 +448,8 @@ def run_ours(args, rank, world, local_rank):
         ach = 11.0 * cpu["block_evals_view0"] / (raster_view0_ms / 1e3) / 1e9
         raster_roof = {"bound": "fp32", "kernel": "raster_rec (T_min records, per-tile sort fused)",
                        "achieved": ach, "peak": peak_gops, "unit": "Gop/s", "frac": ach / peak_gops,
-                       "traffic": RASTER_VIEW0_TRAFFIC,
+                       # captured with 16x16 tiles
+                       "traffic": RASTER_VIEW0_TRAFFIC if (rc.tile_w, rc.tile_h) == (16, 16) else None,
                        "evals_executed": cpu["block_evals_view0"], "evals_unculled": cpu["evals_view0"],
                        "ops_per_eval": 11, "raster_ms": raster_view0_ms,
                        "view": f"view 0 ({cams[0].GetWidth()}x{cams[0].GetHeight()}) rendered alone",
@@ -449,7 +461,8 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": WORKLOAD, "views_per_step": VIEWS, "gaussians": N_GAUSS, "sh_degree": 3,
-                   "termination": "per-pixel T<1e-4", "tiles": "16x16", "keys_per_step": K,
+                   "termination": "per-pixel T<1e-4", "tiles": f"{rc.tile_w}x{rc.tile_h}",
+                   "views_per_block": rc.views_per_block or 16, "autotune": tuned, "keys_per_step": K,
                    "l2": "inputs larger than L2 (scene 672 MB, per-view buffers ~15 GB)", "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "views/s", "h2d_bytes_per_step": VIEWS * 200,
                 "d2h_bytes_per_step": total_bytes},
@@ -479,6 +492,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-plain", action="store_true", help="skip the single-view leg (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg (profiling runs)")
+    ap.add_argument("--no-autotune", action="store_true", help="default knobs (16x16 tiles, 16 views per block)")
     ap.add_argument("--only-ref1024", action="store_true",
                     help="time only the reference-compatible 1024x1024 single-view frame (profiling case)")
     ap.add_argument("--views", type=int, default=VIEWS,

@@ -166,6 +166,47 @@ GS_API int gs_render_batch(gs_ctx* ctx, const gs_scene* scene, const gs_camera* 
 GS_API int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
                          const gs_render_cfg* cfg, uint8_t* h_rgba, gs_stats* stats, void* stream);
 
+/* ---- autotuner (batching knobs per (N, resolution) bucket) ------------- */
+
+/* One timed candidate of gs_autotune. */
+typedef struct gs_tune_result {
+    gs_render_cfg cfg;
+    double ms;      /* median device time of one gs_render_batch call */
+} gs_tune_result;
+
+/* Times gs_render_batch of `cams` with the batching knobs swept over their
+ * valid values and everything else taken from `base`, and stores the
+ * fastest knobs in the context's table under the bucket of (N = the
+ * scene's size, the largest view's pixel count, num_views, base's
+ * termination and ordering); gs_autotune_lookup reads it back.  Swept:
+ *   tile shape 16x16 / 16x8 / 8x8   GS_TERM_TMIN only (the reference mode's
+ *                                   tile-wide termination is defined on the
+ *                                   16x16 tiles it was given; per-pixel
+ *                                   termination gives the same colours for
+ *                                   every shape, while alpha, 255 in tiles
+ *                                   that hold any entry and 0 elsewhere as
+ *                                   in the reference, follows the grid);
+ *   views_per_block 8 / 16 / 32     batches of more than 8 views;
+ *   sort_variant 0..3               GS_ORDER_ONESWEEP only.
+ * Each candidate renders 2 untimed frames (the second captures its graph
+ * when base->graph is set) and then `iterations` timed ones (>= 1) into
+ * context-owned images.  `best` receives base with the winning knobs,
+ * `best_ms` its time; `results` (may be NULL) receives up to
+ * `results_capacity` candidates in the order they were timed and
+ * `num_results` (may be NULL) their count.  Synchronous. */
+GS_API int gs_autotune(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                       const gs_render_cfg* base, int32_t iterations, gs_render_cfg* best, double* best_ms,
+                       gs_tune_result* results, int32_t results_capacity, int32_t* num_results, void* stream);
+/* Applies the knobs gs_autotune stored for the bucket of (n, width*height,
+ * num_views, cfg->termination, cfg->ordering) to *cfg and sets *found = 1;
+ * leaves *cfg as it is and sets *found = 0 when that bucket was not tuned.
+ * Buckets: N and the pixel count by their power of two (floor log2), the
+ * view count by 1, 2-4, 5-8, 9-16, 17-32, 33+. */
+GS_API int gs_autotune_lookup(gs_ctx* ctx, int64_t n, int32_t width, int32_t height, int32_t num_views,
+                              gs_render_cfg* cfg, int32_t* found);
+/* Entries in the context's tuning table. */
+GS_API int32_t gs_autotune_entries(gs_ctx* ctx);
+
 /* ---- performance overlay (app/perf_overlay.cpp:115-161) ---------------- */
 
 /* DrawPerformanceOverlay: draws the reference's eight statistics lines

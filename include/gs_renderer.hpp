@@ -281,6 +281,19 @@ class Renderer {
         return GS_OK;
     }
 
+    // gs_autotune on this camera's view: the options' batching knobs become
+    // the fastest timed ones (tile shape under per-pixel termination), and
+    // the context remembers them for the view's (N, resolution) bucket.
+    int Autotune(const Camera& camera, int iterations = 3)
+    {
+        if (!ctx_ || !scene_) return GS_ERR_INVALID;
+        gs_render_cfg best{};
+        const int rc = gs_autotune(ctx_, scene_, &camera.Native(), 1, &cfg_, iterations, &best, nullptr, nullptr, 0,
+                                   nullptr, nullptr);
+        if (rc == GS_OK) cfg_ = best;
+        return rc;
+    }
+
   private:
     int EnsureCtx() { return ctx_ ? GS_OK : gs_ctx_create(0, &ctx_); }
 

@@ -1,7 +1,7 @@
 // Drives the C++ renderer API (include/gs_renderer.hpp) the way a caller of
 // the reference's core/renderer.h would: LoadPly -> UploadModel -> Render
 // into a device RGBA buffer, then writes the image bytes to a file.
-//   renderer_api_main <ply> <out.raw> <width> <height> <reference-mode 0|1>
+//   renderer_api_main <ply> <out.raw> <width> <height> <reference-mode 0|1> [autotune 0|1]
 #include <cstdio>
 #include <cstdlib>
 #include <vector>
@@ -34,6 +34,10 @@ int main(int argc, char** argv)
         renderer.SetConfig(cfg);
     }
     if (renderer.UploadModel(model) != GS_OK) return 4;
+    if (argc > 6 && std::atoi(argv[6])) {
+        if (renderer.Autotune(cam) != GS_OK) return 8;
+        std::printf("tuned tile %dx%d\n", renderer.Config().tile_w, renderer.Config().tile_h);
+    }
     uint8_t* d = nullptr;
     if (cudaMalloc(&d, (size_t)w * h * 4) != cudaSuccess) return 5;
     gauss_render::RenderStats stats;

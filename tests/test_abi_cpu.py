@@ -65,6 +65,9 @@ def test_errors_without_gpu(gs):
     # null arguments are rejected before any device work
     assert gs.lib.gs_render(None, None, None, None, None, None, None) == gs.GS_ERR_INVALID
     assert gs.lib.gs_stage_ranges(-1, None, 0, None, None) == gs.GS_ERR_INVALID
+    assert gs.lib.gs_autotune(None, None, None, 0, None, 1, None, None, None, 0, None, None) == gs.GS_ERR_INVALID
+    assert gs.lib.gs_autotune_lookup(None, 0, 1, 1, 1, None, None) == gs.GS_ERR_INVALID
+    assert gs.lib.gs_autotune_entries(None) == 0
 
 
 def test_overlay_text_matches_reference_formats(gs):
