@@ -181,11 +181,14 @@ typedef struct gs_tune_result {
  * termination and ordering); gs_autotune_lookup reads it back.  Swept:
  *   tile shape 16x16 / 16x8 / 8x8   GS_TERM_TMIN only (the reference mode's
  *                                   tile-wide termination is defined on the
- *                                   16x16 tiles it was given; per-pixel
- *                                   termination gives the same colours for
- *                                   every shape, while alpha, 255 in tiles
- *                                   that hold any entry and 0 elsewhere as
- *                                   in the reference, follows the grid);
+ *                                   16x16 tiles it was given; under
+ *                                   per-pixel termination the colours of
+ *                                   every shape agree to a few 8-bit steps
+ *                                   at most, from splats whose faint tails
+ *                                   reach past their tiles, while alpha,
+ *                                   255 in tiles that hold any entry and 0
+ *                                   elsewhere as in the reference, follows
+ *                                   the grid);
  *   views_per_block 8 / 16 / 32     batches of more than 8 views;
  *   sort_variant 0..3               GS_ORDER_ONESWEEP only.
  * Each candidate renders 2 untimed frames (the second captures its graph
