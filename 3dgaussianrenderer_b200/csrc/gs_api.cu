@@ -112,6 +112,7 @@ struct FrameGraph {
     int seen = 0;                    // calls with this key
     int failed = 0;                  // capture failed: run this key without a graph
     int raster_groups = 0;           // raster launched per view group (host-output batches)
+    int split = 0;                   // needed 2^31 tile keys or more: render as halves of the views
 };
 constexpr size_t kMaxGraphs = 8;
 // gs_render_batch_host renders batches of more than this many views in
@@ -143,6 +144,11 @@ struct TuneEntry {
 constexpr size_t kMaxTuneEntries = 256;
 
 std::atomic<uint64_t> g_scene_uid{1};
+
+// Internal status of a frame whose tile lists need 2^31 entries or more
+// (list positions are int32): run_frame renders it again as two frames
+// over halves of its views.
+constexpr int kSplitViews = -2;
 
 }  // namespace
 
@@ -407,7 +413,7 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     GS_CUDA(cudaStreamSynchronize(st));
     if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "projection look-back timed out");
     const int64_t K = n > 0 ? ctx->h_counters->total : 0;
-    if (K >= (1ll << 31)) return fail(GS_ERR_CAPACITY, "more than 2^31 tile keys");
+    if (K >= (1ll << 31)) return fail(kSplitViews, "more than 2^31 tile keys");
 
     // 2. emit keys
     if (K > ctx->key_capacity) {
@@ -811,6 +817,7 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         }
         g->last_use = ++ctx->use_clock;
         ++g->seen;
+        if (g->split) return kSplitViews;
     }
 
     int attempts = 0;
@@ -850,7 +857,10 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
             return fail(GS_ERR_DEVICE_TIMEOUT, "frame look-back timed out");
         }
         const int64_t K = ctx->h_counters->total;
-        if (K >= (1ll << 31)) return fail(GS_ERR_CAPACITY, "more than 2^31 tile keys");
+        if (K >= (1ll << 31)) {
+            if (g) g->split = 1;
+            return fail(kSplitViews, "more than 2^31 tile keys");
+        }
         if (!ctx->h_counters->overflow) break;
         if (attempts >= 2) return fail(GS_ERR_CUDA, "tile list overflow after regrowing");
         if (g) drop_graph(*g);
@@ -877,13 +887,51 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
 }
 
 int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
+              uint8_t* const* outs, gs_stats* stats, cudaStream_t st);
+
+// Views are independent, so a batch renders as frames over parts of its
+// views with the same images: halves, as long as the tile lists or the
+// (view, Gaussian) items would need 2^31 entries or more.
+int run_frame_halves(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views,
+                     const gs_render_cfg& cfg, uint8_t* const* outs, gs_stats* stats, cudaStream_t st, int tried)
+{
+    const int h = num_views / 2;
+    gs_stats a{}, b{};
+    int rc = run_frame(ctx, scene, cams, h, cfg, outs, &a, st);
+    if (rc) return rc;
+    rc = run_frame(ctx, scene, cams + h, num_views - h, cfg, outs + h, &b, st);
+    if (rc) return rc;
+    if (stats) {
+        stats->sh_eval_ms = a.sh_eval_ms + b.sh_eval_ms;
+        stats->project_ms = a.project_ms + b.project_ms;
+        stats->build_tile_ms = a.build_tile_ms + b.build_tile_ms;
+        stats->sort_ms = a.sort_ms + b.sort_ms;
+        stats->raster_ms = a.raster_ms + b.raster_ms;
+        stats->total_ms = a.total_ms + b.total_ms;
+        stats->num_keys = a.num_keys + b.num_keys;
+        stats->num_tiles = a.num_tiles + b.num_tiles;
+        stats->kernel_launches = a.kernel_launches + b.kernel_launches;
+        stats->graph_replay = a.graph_replay && b.graph_replay;
+        stats->attempts = tried + std::max(a.attempts, b.attempts);
+    }
+    return GS_OK;
+}
+
+int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
               uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
 {
+    if (num_views > 1 && scene && scene->n * (int64_t)num_views >= (1ll << 31))
+        return run_frame_halves(ctx, scene, cams, num_views, cfg, outs, stats, st, 0);
+    int rc;
     if (cfg.ordering == GS_ORDER_ONESWEEP) {
         if (stats) stats->graph_replay = 0, stats->attempts = 1;
-        return run_frame_onesweep(ctx, scene, cams, num_views, cfg, outs, stats, st);
+        rc = run_frame_onesweep(ctx, scene, cams, num_views, cfg, outs, stats, st);
+    } else {
+        rc = run_frame_bucket(ctx, scene, cams, num_views, cfg, outs, stats, st);
     }
-    return run_frame_bucket(ctx, scene, cams, num_views, cfg, outs, stats, st);
+    if (rc != kSplitViews) return rc;
+    if (num_views == 1) return fail(GS_ERR_CAPACITY, "more than 2^31 tile keys in one view");
+    return run_frame_halves(ctx, scene, cams, num_views, cfg, outs, stats, st, 1);
 }
 
 // floor(log2(x)) for x >= 1, -1 for x <= 0
@@ -1343,9 +1391,12 @@ int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* ca
         }
         const int rc = run_frame_bucket(ctx, scene, cams, num_views, *cfg, outs.data(), stats, st, &hc);
         const cudaError_t se = cudaStreamSynchronize(ctx->copy_stream);
-        if (rc) return rc;
-        if (se != cudaSuccess) return cuda_fail(se, "image copy");
-        return GS_OK;
+        if (rc != kSplitViews) {
+            if (rc) return rc;
+            if (se != cudaSuccess) return cuda_fail(se, "image copy");
+            return GS_OK;
+        }
+        // too many tile keys for one frame: render in chunks below
     }
     // Other frames render in chunks of kHostChunkViews views; each chunk's
     // images are copied to the host on a second stream while the next chunk

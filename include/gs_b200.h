@@ -94,7 +94,10 @@ typedef struct gs_stats {
     int64_t num_tiles;
     int64_t kernel_launches; /* gs_b200 kernels launched for the frame */
     int32_t graph_replay;    /* 1: the frame ran as a replay of a captured CUDA graph */
-    int32_t attempts;        /* launches of the frame: 2 when the tile list outgrew its buffers and was redone */
+    int32_t attempts;        /* launches of the frame: 2 when the tile list outgrew its buffers and was redone;
+                                a batch whose tile lists need 2^31 entries or more (or whose views x Gaussians
+                                reach 2^31) renders as frames over halves of its views, with the same images:
+                                the halves' stats add up and attempts counts the frame that found it too big */
 } gs_stats;
 
 typedef struct gs_ctx gs_ctx;
