@@ -219,6 +219,42 @@ def test_full_frame_vs_oracle(gs, ctx, O, W, H, tw, th):
     assert psnr(img, oimg) >= 45.0
 
 
+@pytest.mark.parametrize("config", ["plain100k", "plain1m"])
+def test_plain_configs_full_size_vs_oracle(gs, ctx, O, config):
+    """The two single-view configurations at their full sizes: 100k uniform
+    Gaussians at 800x800 from (0, 0, 3), fovy 60; 1M clustered Gaussians at
+    1920x1080 from a seeded pose on a radius-10 sphere, fovy 50.  Tile lists
+    of the GPU's projected floats are bit-exact in the oracle's build; whole
+    frames in both modes meet the end-to-end image bar."""
+    sc = gs.scenes.config_scene(config)
+    if config == "plain100k":
+        cam = gs.look_at((0.0, 0.0, 3.0), (0, 0, 0), (0, 1, 0), 60.0, 800, 800, 0.1, 100.0)
+    else:
+        eye = gs.scenes.sphere_pose(np.random.default_rng(12), 10.0)
+        cam = gs.look_at(eye, (0, 0, 0), (0, 1, 0), 50.0, 1920, 1080, 0.1, 100.0)
+    n = sc["pos4"].shape[0]
+    rc = gs.RenderConfig.reference()
+    xy, z, ell, _ = project_gpu(gs, sc["pos4"], sc["sr4"], cam)
+    keys = torch.zeros(64 * n, dtype=torch.int64, device="cuda")
+    vals = torch.zeros(64 * n, dtype=torch.int32, device="cuda")
+    K = gs.stage_build(ctx, n, xy, z, ell, cam, rc, keys, vals, 64 * n)
+    ok, ov = O.build(xy.cpu().numpy(), ell.cpu().numpy(), z.cpu().numpy(), cam, rc)
+    assert K == len(ok) > 0
+    assert np.array_equal(keys[:K].cpu().numpy().view(np.uint64), ok)
+    assert np.array_equal(vals[:K].cpu().numpy(), ov)
+    del keys, vals
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    for mode_cfg in (gs.RenderConfig.reference(), gs.RenderConfig()):
+        img, st = gs.render_host(ctx, scene, cam, mode_cfg)
+        oimg, OK, _, _ = O.render(sc, sh, cam, mode_cfg)
+        assert abs(st["num_keys"] - OK) <= max(4, OK // 2000)
+        diff = np.abs(img.astype(int) - oimg.astype(int))
+        assert np.percentile(diff, 99.9) <= IMG_TOL, mode_cfg.termination
+        assert psnr(img, oimg) >= 45.0
+    scene.close()
+
+
 def test_batch_views_identical_to_single(gs, ctx):
     """Every view of a mixed-resolution batch is bit-identical to rendering it alone."""
     sc = gs.scenes.cluster_scene(150_000, 32, 5.0, seed=77)
