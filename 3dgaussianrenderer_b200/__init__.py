@@ -620,11 +620,13 @@ def load_ply(path: str) -> dict:
     if lib.gs_ply_info(path.encode(), ctypes.byref(n), ctypes.byref(deg)) != GS_OK:
         raise ValueError(lib.gs_ply_last_error().decode())
     n, deg = int(n.value), int(deg.value)
-    pos4 = np.zeros((n, 4), np.float32)
-    sr4 = np.zeros((n, 4), np.float32)
-    color4 = np.zeros((n, 4), np.float32)
+    # every element is written by gs_ply_read (the last SH group's padding
+    # included): no zero fill
+    pos4 = np.empty((n, 4), np.float32)
+    sr4 = np.empty((n, 4), np.float32)
+    color4 = np.empty((n, 4), np.float32)
     groups = (n + 255) // 256
-    sh = np.zeros(groups * 256 * 3 * (deg + 1) ** 2, np.float32) if deg > 0 else None
+    sh = np.empty(groups * 256 * 3 * (deg + 1) ** 2, np.float32) if deg > 0 else None
     bounds = np.zeros(6, np.float32)
     if lib.gs_ply_read(path.encode(), _ptr(pos4), _ptr(sr4), _ptr(color4), _ptr(sh), _ptr(bounds)) != GS_OK:
         raise ValueError(lib.gs_ply_last_error().decode())

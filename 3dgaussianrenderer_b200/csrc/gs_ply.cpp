@@ -1,9 +1,10 @@
 // PLY ingest and export for gs_b200 (replaces parsePly/savePly,
 // core/ply_parser.cpp:15-393, and LoadPly, core/ply_loader.cpp:105-278).
 //
-// The file is read with one sequential read into memory and the vertex
-// records are transformed in parallel (one std::thread per hardware
-// thread over contiguous vertex ranges), straight into the device
+// The file is memory-mapped (no copy of the vertex data, no zero-filled
+// staging buffer) and the vertex records are transformed in parallel (one
+// std::thread per hardware thread over contiguous vertex ranges, each
+// faulting in its own part of the file), straight into the device
 // layouts: position/opacity, scale + quantised rotation, DC colour, and
 // the SH coefficients interleaved per coefficient and regrouped by 256
 // (app/main.cpp:147-177).  The per-vertex transforms are the reference's:
@@ -23,6 +24,11 @@
 #include <string>
 #include <thread>
 #include <vector>
+
+#include <fcntl.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 namespace {
 
@@ -142,26 +148,57 @@ void parallel_for(int64_t n, F&& f)
     for (auto& x : th) x.join();
 }
 
+// A read-only mapping of the whole file; the vertex data starts at
+// `data`, at any byte offset (values are read with memcpy).
 struct PlyFile {
     PlyHeader h;
     Layout L;
-    std::vector<float> data;  // count x props
+    const char* map = nullptr;
+    size_t map_bytes = 0;
+    const char* data = nullptr;  // count x props little-endian floats
+    PlyFile() = default;
+    PlyFile(const PlyFile&) = delete;
+    PlyFile& operator=(const PlyFile&) = delete;
+    ~PlyFile()
+    {
+        if (map) munmap(const_cast<char*>(map), map_bytes);
+    }
+    // property k of vertex i
+    float at(int64_t i, int k) const
+    {
+        float v;
+        std::memcpy(&v, data + ((size_t)i * h.props.size() + (size_t)k) * sizeof(float), sizeof(float));
+        return v;
+    }
 };
 
-PlyFile read_ply(const char* path, bool with_data)
+void read_ply(const char* path, bool with_data, PlyFile& f)
 {
-    std::ifstream in(path, std::ios::binary);
-    if (!in.is_open()) throw std::invalid_argument(std::string("cannot open ") + path);
-    PlyFile f;
-    f.h = parse_header(in);
-    f.L = layout_of(f.h);
-    if (with_data) {
-        const size_t nfl = (size_t)f.h.count * f.h.props.size();
-        f.data.resize(nfl);
-        in.read(reinterpret_cast<char*>(f.data.data()), (std::streamsize)(nfl * sizeof(float)));
-        if ((size_t)in.gcount() != nfl * sizeof(float)) throw std::invalid_argument("truncated vertex data");
+    {
+        std::ifstream in(path, std::ios::binary);
+        if (!in.is_open()) throw std::invalid_argument(std::string("cannot open ") + path);
+        f.h = parse_header(in);
     }
-    return f;
+    f.L = layout_of(f.h);
+    if (!with_data) return;
+    const size_t bytes = (size_t)f.h.count * f.h.props.size() * sizeof(float);
+    const int fd = open(path, O_RDONLY);
+    if (fd < 0) throw std::invalid_argument(std::string("cannot open ") + path);
+    struct stat sb;
+    if (fstat(fd, &sb) != 0 || (size_t)sb.st_size < f.h.data_offset + bytes) {
+        close(fd);
+        throw std::invalid_argument("truncated vertex data");
+    }
+    if (bytes == 0) {
+        close(fd);
+        return;
+    }
+    void* m = mmap(nullptr, (size_t)sb.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+    close(fd);  // the mapping keeps the file
+    if (m == MAP_FAILED) throw std::invalid_argument(std::string("cannot map ") + path);
+    f.map = static_cast<const char*>(m);
+    f.map_bytes = (size_t)sb.st_size;
+    f.data = f.map + f.h.data_offset;
 }
 
 }  // namespace
@@ -172,7 +209,8 @@ GS_API int gs_ply_info(const char* path, int64_t* out_n, int32_t* out_sh_degree)
 {
     try {
         if (!path) return GS_ERR_INVALID;
-        PlyFile f = read_ply(path, false);
+        PlyFile f;
+        read_ply(path, false, f);
         if (out_n) *out_n = f.h.count;
         if (out_sh_degree) *out_sh_degree = f.L.degree;
         return GS_OK;
@@ -189,18 +227,17 @@ GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotat
 {
     try {
         if (!path) return GS_ERR_INVALID;
-        PlyFile f = read_ply(path, true);
+        PlyFile f;
+        read_ply(path, true, f);
         const int64_t n = f.h.count;
-        const size_t np = f.h.props.size();
         const Layout& L = f.L;
-        const float* D = f.data.data();
         const int sc = L.sh_count;
         const int rgb = (sc - 3) / 3;
         parallel_for(n, [&](int64_t lo, int64_t hi) {
             for (int64_t i = lo; i < hi; ++i) {
-                const float* r = D + (size_t)i * np;
+                const auto r = [&f, i](int k) { return f.at(i, k); };
                 // glm::quat(w = rot_0, x = rot_1, y = rot_2, z = rot_3), normalised
-                float qw = r[L.off[3]], qx = r[L.off[4]], qy = r[L.off[5]], qz = r[L.off[6]];
+                float qw = r(L.off[3]), qx = r(L.off[4]), qy = r(L.off[5]), qz = r(L.off[6]);
                 const float len = std::sqrt((qw * qw + qx * qx) + (qy * qy + qz * qz));
                 if (len <= 0.0f) {
                     qw = 1.0f;
@@ -212,19 +249,19 @@ GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotat
                     qy *= inv;
                     qz *= inv;
                 }
-                const float opacity = sigmoidf(r[L.off[13]]);
+                const float opacity = sigmoidf(r(L.off[13]));
                 if (h_position) {
                     float* p = h_position + 4 * i;
-                    p[0] = r[L.off[0]];
-                    p[1] = r[L.off[1]];
-                    p[2] = r[L.off[2]];
+                    p[0] = r(L.off[0]);
+                    p[1] = r(L.off[1]);
+                    p[2] = r(L.off[2]);
                     p[3] = opacity;
                 }
                 if (h_scale_rotation) {
                     float* s = h_scale_rotation + 4 * i;
-                    s[0] = std::exp(r[L.off[7]]);
-                    s[1] = std::exp(r[L.off[8]]);
-                    s[2] = std::exp(r[L.off[9]]);
+                    s[0] = std::exp(r(L.off[7]));
+                    s[1] = std::exp(r(L.off[8]));
+                    s[2] = std::exp(r(L.off[9]));
                     const uint32_t bits = encode_vec4((qx + 1.0f) * 0.5f, (qy + 1.0f) * 0.5f, (qz + 1.0f) * 0.5f,
                                                       (qw + 1.0f) * 0.5f);
                     std::memcpy(&s[3], &bits, 4);
@@ -232,9 +269,9 @@ GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotat
                 if (h_color) {
                     const float C0 = 0.28209479177387814f;
                     float* c = h_color + 4 * i;
-                    c[0] = r[L.off[10]] * C0 + 0.5f;
-                    c[1] = r[L.off[11]] * C0 + 0.5f;
-                    c[2] = r[L.off[12]] * C0 + 0.5f;
+                    c[0] = r(L.off[10]) * C0 + 0.5f;
+                    c[1] = r(L.off[11]) * C0 + 0.5f;
+                    c[2] = r(L.off[12]) * C0 + 0.5f;
                     c[3] = opacity;
                 }
                 if (h_sh_grouped && L.degree > 0) {
@@ -242,11 +279,11 @@ GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotat
                     // f_rest is channel-major in the file (ply_parser.cpp:332-348)
                     const int64_t g = i / 256, t = i % 256;
                     float* base = h_sh_grouped + (size_t)g * 256 * sc + t;
-                    base[0 * 256] = r[L.off[10]];
-                    base[1 * 256] = r[L.off[11]];
-                    base[2 * 256] = r[L.off[12]];
+                    base[0 * 256] = r(L.off[10]);
+                    base[1 * 256] = r(L.off[11]);
+                    base[2 * 256] = r(L.off[12]);
                     for (int j = 0; j < rgb; ++j)
-                        for (int c = 0; c < 3; ++c) base[(size_t)(3 + 3 * j + c) * 256] = r[L.rest[c * rgb + j]];
+                        for (int c = 0; c < 3; ++c) base[(size_t)(3 + 3 * j + c) * 256] = r(L.rest[c * rgb + j]);
                 }
             }
         });
@@ -268,7 +305,7 @@ GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotat
             }
             for (int64_t i = 0; i < n; ++i)
                 for (int c = 0; c < 3; ++c) {
-                    const float v = D[(size_t)i * np + L.off[c]];
+                    const float v = f.at(i, L.off[c]);
                     mn[c] = (v < mn[c]) ? v : mn[c];
                     mx[c] = (mx[c] < v) ? v : mx[c];
                 }
