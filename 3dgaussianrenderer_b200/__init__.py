@@ -127,6 +127,8 @@ _sig("gs_scene_create", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.POINTER(_P))
 _sig("gs_draw_stats", _I, _P, _I32, _I32, _I64, ctypes.POINTER(gs_stats), ctypes.c_double, _P)
 _sig("gs_format_stats", _I, _I64, ctypes.POINTER(gs_stats), ctypes.c_double, ctypes.c_char_p, _I32)
 _sig("gs_font_glyph", _I, _I32, ctypes.POINTER(ctypes.c_uint8))
+_sig("gs_write_ppm", _I, ctypes.c_char_p, _P, _I32, _I32)
+_sig("gs_write_png", _I, ctypes.c_char_p, _P, _I32, _I32)
 _sig("gs_scene_create_ex", _I, _P, _I64, _P, _P, _P, _P, _I32, ctypes.c_uint32, ctypes.POINTER(_P))
 _sig("gs_scene_destroy", _I, _P)
 _sig("gs_scene_size", _I64, _P)
@@ -488,6 +490,17 @@ def format_stats(num_gaussians: int, stats: dict, fps: float) -> str:
     buf = ctypes.create_string_buffer(1024)
     check(lib.gs_format_stats(num_gaussians, ctypes.byref(st), float(fps), buf, len(buf)), "gs_format_stats")
     return buf.value.decode()
+
+
+def write_image(path: str, rgba: np.ndarray) -> None:
+    """Writes a host RGBA8 frame (H x W x 4, row 0 at the bottom as rendered)
+    as .ppm or .png, top row first."""
+    img = np.ascontiguousarray(rgba, np.uint8)
+    if img.ndim != 3 or img.shape[2] != 4:
+        raise ValueError("expected an H x W x 4 uint8 image")
+    H, W = img.shape[:2]
+    fn = lib.gs_write_png if path.lower().endswith(".png") else lib.gs_write_ppm
+    check(fn(path.encode(), img.ctypes.data, W, H), "gs_write_png" if fn is lib.gs_write_png else "gs_write_ppm")
 
 
 def font_glyph(c: str) -> list:

@@ -229,6 +229,16 @@ GS_API int gs_format_stats(int64_t num_gaussians, const gs_stats* stats, double 
  * all zero outside ASCII 32..126). */
 GS_API int gs_font_glyph(int32_t c, uint8_t rows[7]);
 
+/* ---- headless image output (replaces the PBO display path,
+ *      core/utilities.h:110-153, app/opengl_display.cpp) --------------- */
+
+/* Write a host RGBA8 frame (W x H, row 0 at the bottom, as rendered) to a
+ * file with the top row first: binary PPM (P6, RGB; alpha dropped) or PNG
+ * (8-bit RGBA, uncompressed deflate blocks).  GS_ERR_INVALID on a bad
+ * argument or a failed write. */
+GS_API int gs_write_ppm(const char* path, const uint8_t* h_rgba, int32_t width, int32_t height);
+GS_API int gs_write_png(const char* path, const uint8_t* h_rgba, int32_t width, int32_t height);
+
 /* ---- stage API (core/gaussian_render.cuh:113-126) ---------------------- */
 /* Explicit-argument replacements of the reference's constant-memory stage
  * functions.  All pointers are device pointers; every call is asynchronous

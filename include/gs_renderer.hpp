@@ -11,6 +11,8 @@
 //                               that core/renderer.cpp:18,28 calls)
 //   gauss_render::Renderer      core/renderer.h:13-50
 //   gauss_render::DrawPerformanceOverlay  app/perf_overlay.h:9-15
+//   gauss_render::SaveImage     (headless: the frame to a PNG/PPM file in place
+//                               of the OpenGL display, app/opengl_display.cpp)
 // Vector arguments accept any type with x/y/z members (glm::vec3 included).
 // Renderer::Render writes RGBA8 into a device buffer, like the reference's
 // mapped PBO (row 0 = bottom).  Errors are reported through the int
@@ -346,6 +348,17 @@ inline int DrawPerformanceOverlay(uint8_t* buffer, int width, int height, int nu
     s.raster_ms = stats.raster_ms;
     s.total_ms = stats.total_ms;
     return gs_draw_stats(buffer, width, height, num_gaussians, &s, fps, stream);
+}
+
+// Headless stand-in for the reference's on-screen display: writes a host
+// RGBA8 frame (row 0 = bottom, as Render leaves it) to `path`, top row
+// first, as PNG when the name ends in ".png", else as binary PPM.
+inline int SaveImage(const std::string& path, const uint8_t* host_rgba, int width, int height)
+{
+    const bool png = path.size() >= 4 && (path.compare(path.size() - 4, 4, ".png") == 0 ||
+                                          path.compare(path.size() - 4, 4, ".PNG") == 0);
+    return png ? gs_write_png(path.c_str(), host_rgba, width, height)
+               : gs_write_ppm(path.c_str(), host_rgba, width, height);
 }
 
 }  // namespace gauss_render

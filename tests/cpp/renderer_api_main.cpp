@@ -4,6 +4,7 @@
 //   renderer_api_main <ply> <out.raw> <width> <height> <reference-mode 0|1> [autotune 0|1]
 #include <cstdio>
 #include <cstdlib>
+#include <string>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -49,6 +50,7 @@ int main(int argc, char** argv)
     if (!f) return 7;
     std::fwrite(img.data(), 1, img.size(), f);
     std::fclose(f);
+    if (gauss_render::SaveImage(std::string(argv[2]) + ".png", img.data(), w, h) != GS_OK) return 9;
     std::printf("stats project %.3f build %.3f sort %.3f raster %.3f total %.3f ms\n", stats.project_ms,
                 stats.build_tile_ms, stats.sort_ms, stats.raster_ms, stats.total_ms);
     return 0;

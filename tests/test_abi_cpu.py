@@ -88,3 +88,48 @@ def test_overlay_font(gs):
     # every character the overlay prints has a glyph
     for c in "FPS:.0123456789GaussinTotalHProjectBuildSortRasterm":
         assert any(gs.font_glyph(c)), c
+
+
+def test_image_writers_flip_rows_and_round_trip(gs, tmp_path):
+    """PPM and PNG output: top row first (the frame's row 0 is the bottom),
+    PPM drops alpha, PNG keeps RGBA; every PNG chunk CRC and the zlib
+    stream check out with the standard library's decoders."""
+    import struct
+    import zlib
+    rng = np.random.default_rng(4)
+    H, W = 23, 37
+    img = rng.integers(0, 256, (H, W, 4), dtype=np.uint8)
+    ppm = str(tmp_path / "f.ppm")
+    gs.write_image(ppm, img)
+    data = open(ppm, "rb").read()
+    head = f"P6\n{W} {H}\n255\n".encode()
+    assert data.startswith(head)
+    rgb = np.frombuffer(data[len(head):], np.uint8).reshape(H, W, 3)
+    assert np.array_equal(rgb, img[::-1, :, :3])
+    png = str(tmp_path / "f.png")
+    gs.write_image(png, img)
+    data = open(png, "rb").read()
+    assert data[:8] == b"\x89PNG\r\n\x1a\n"
+    pos, chunks = 8, {}
+    while pos < len(data):
+        (n,) = struct.unpack(">I", data[pos:pos + 4])
+        kind, body = data[pos + 4:pos + 8], data[pos + 8:pos + 8 + n]
+        (crc,) = struct.unpack(">I", data[pos + 8 + n:pos + 12 + n])
+        assert crc == zlib.crc32(kind + body)
+        chunks[kind] = chunks.get(kind, b"") + body
+        pos += 12 + n
+    assert struct.unpack(">IIBBBBB", chunks[b"IHDR"]) == (W, H, 8, 6, 0, 0, 0)
+    raw = np.frombuffer(zlib.decompress(chunks[b"IDAT"]), np.uint8).reshape(H, 1 + 4 * W)
+    assert (raw[:, 0] == 0).all()
+    assert np.array_equal(raw[:, 1:].reshape(H, W, 4), img[::-1])
+    assert b"IEND" in chunks
+    # a frame larger than one stored deflate block
+    big = rng.integers(0, 256, (300, 200, 4), dtype=np.uint8)
+    gs.write_image(png, big)
+    data = open(png, "rb").read()
+    idat = data.index(b"IDAT")
+    (n,) = struct.unpack(">I", data[idat - 4:idat])
+    raw = np.frombuffer(zlib.decompress(data[idat + 4:idat + 4 + n]), np.uint8).reshape(300, 801)
+    assert np.array_equal(raw[:, 1:].reshape(300, 200, 4), big[::-1])
+    with pytest.raises(gs.GsError):
+        gs.write_image(str(tmp_path / "no_such_dir" / "x.png"), img)

@@ -32,6 +32,7 @@ def test_cpp_renderer_api_matches_c_abi(gs, tmp_path):
         r = subprocess.run([exe, ply, out, "640", "480", str(ref_mode)], capture_output=True, text=True)
         assert r.returncode == 0, r.stdout + r.stderr
         img = np.fromfile(out, np.uint8).reshape(480, 640, 4)
+        assert os.path.getsize(out + ".png") > 640 * 480 * 4  # gauss_render::SaveImage, uncompressed
         cam = gs.look_at((0.3, 0.2, 3.0), (0, 0, 0), (0, 1, 0), 60.0, 640, 480, 0.1, 100.0)
         rc = gs.RenderConfig.reference() if ref_mode else gs.RenderConfig()
         want, _ = gs.render_host(ctx, scene, cam, rc)
