@@ -1384,11 +1384,14 @@ int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* ca
         hc.h_rgba = h_rgba;
         hc.copy = ctx->copy_stream;
         hc.groups = std::min(kMaxRasterGroups, (num_views + kHostGroupViews - 1) / kHostGroupViews);
-        const int per = (num_views + hc.groups - 1) / hc.groups;
-        for (int g = 0; g <= hc.groups; ++g) {
-            hc.first_view[g] = std::min(num_views, g * per);
+        // the last group's copy is the one nothing overlaps: a quarter of a
+        // group's views, the others share the rest evenly
+        const int last = std::max(1, (num_views + hc.groups - 1) / hc.groups / 4);
+        const int per = (num_views - last + hc.groups - 2) / (hc.groups - 1);
+        for (int g = 0; g < hc.groups; ++g) hc.first_view[g] = std::min(num_views - last, g * per);
+        hc.first_view[hc.groups] = num_views;
+        for (int g = 0; g <= hc.groups; ++g)
             hc.first_byte[g] = hc.first_view[g] < num_views ? offs[hc.first_view[g]] : total;
-        }
         const int rc = run_frame_bucket(ctx, scene, cams, num_views, *cfg, outs.data(), stats, st, &hc);
         const cudaError_t se = cudaStreamSynchronize(ctx->copy_stream);
         if (rc != kSplitViews) {
