@@ -408,7 +408,32 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
         const int clear = ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
         if (clear >= 0) return clear != 0;
     }
-    const float iex = FAST ? rcp_approx(e.ex) : 0.0f, iey = FAST ? rcp_approx(e.ey) : 0.0f;
+    if constexpr (FAST) {
+        // The same five tests on the tile's image in ellipse coordinates, a
+        // parallelogram: corner (x0, y0) maps to a, the x edge to u, the y
+        // edge to v, so the other corners are sums and each edge's squared
+        // length is |u|^2 or |v|^2.
+        const float iex = rcp_approx(e.ex), iey = rcp_approx(e.ey);
+        const float dx0 = x0 - e.cx, dy0 = y0 - e.cy;
+        const float ax = (dx0 * e.cs + dy0 * e.sn) * iex, ay = (dy0 * e.cs - dx0 * e.sn) * iey;
+        const float w = x1 - x0, h = y1 - y0;
+        const float ux = (w * e.cs) * iex, uy = -(w * e.sn) * iey;
+        const float vx = (h * e.sn) * iex, vy = (h * e.cs) * iey;
+        const float rx = ax + 0.5f * (ux + vx), ry = ay + 0.5f * (uy + vy);
+        if (len2(rx, ry) < 1.0f) return true;
+        const float iu = rcp_approx(len2(ux, uy)), iv = rcp_approx(len2(vx, vy));
+        const float bx = ax + ux, by = ay + uy;  // (x1, y0)
+        const float cx = bx + vx, cy = by + vy;  // (x1, y1)
+        const float qx = ax + vx, qy = ay + vy;  // (x0, y1)
+        // segment p + t d, t in [0, 1]: its point nearest the origin inside the unit circle
+        auto edge = [](const float px, const float py, const float dx, const float dy, const float inv) {
+            const float t = __saturatef(-(px * dx + py * dy) * inv);
+            return len2(px + t * dx, py + t * dy) < 1.0f;
+        };
+        return edge(ax, ay, ux, uy, iu) || edge(bx, by, vx, vy, iv) || edge(cx, cy, -ux, -uy, iu) ||
+               edge(qx, qy, -vx, -vy, iv);
+    }
+    const float iex = 0.0f, iey = 0.0f;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
     const float rcy = y0 + (y1 - y0) * 0.5f;
