@@ -415,13 +415,15 @@ def run_ours(args, rank, world, local_rank):
     K = keys
     # Frame kernel against HBM.  Algorithmic bytes of one launch: the scene
     # (32 B position + scale/rotation, 12 (d + 1)^2 = 192 B SH per Gaussian)
-    # read once per block of 16 views, and the 48-byte splat record per
-    # (view, Gaussian) of the scope table written: ceil(V / 16) N 224 + V N 48.
-    # traffic: DRAM bytes of an ncu capture of a 4-view frame (672.7 MB read,
-    # 509.2 MB written), scaled to 64 views (reads per 16 views, writes per
-    # view).  The kernel is issue-bound, far under this roof.
-    alg_frame = ((VIEWS + 15) // 16) * N_GAUSS * (32 + 12 * 16) + VIEWS * N_GAUSS * 48
-    frame_traffic = 672.7e6 * ((VIEWS + 15) // 16) + 509.2e6 / 4 * VIEWS if VIEWS == 64 else None
+    # read once per block of `vpb` views, and the 48-byte splat record per
+    # (view, Gaussian) of the scope table written: ceil(V / vpb) N 224 + V N 48.
+    # traffic: DRAM bytes of an ncu capture of a 4-view frame (684.2 MB read,
+    # 506.1 MB written), scaled to 64 views (reads per block of views, writes
+    # per view).  The kernel is issue-bound, far under this roof.
+    vpb = min(VIEWS, rc.views_per_block or 16)
+    blocks = (VIEWS + vpb - 1) // vpb
+    alg_frame = blocks * N_GAUSS * (32 + 12 * 16) + VIEWS * N_GAUSS * 48
+    frame_traffic = 684.2e6 * blocks + 506.1e6 / 4 * VIEWS if VIEWS == 64 else None
     frame_gbs = alg_frame / (per["project_ms"] / 1e3) / 1e9 if per["project_ms"] > 0 else None
     frame_roof = {"bound": "hbm", "kernel": "frame_project (SH + projection + tile counts)",
                   "achieved": frame_gbs, "peak": hbm, "unit": "GB/s",
