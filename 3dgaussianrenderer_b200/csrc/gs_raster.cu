@@ -485,10 +485,9 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
 {
     constexpr int NW = TW * TH / 64;
     constexpr int WX = TW / 8;
-    __shared__ float4 s_s[NW][32];
-    __shared__ ulonglong2 s_yc[NW][32];
-    __shared__ ulonglong2 s_rg[NW][32];
-    __shared__ f2 s_bl[NW][32];
+    __shared__ float4 s_s[NW][32];  // (x, A, B, L)
+    __shared__ float4 s_q[NW][32];  // (y, C, red, green)
+    __shared__ float s_b[NW][32];   // blue
     __shared__ FusedSortSmem<TW * TH / 2> fs;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : a.tile_base + (int64_t)blockIdx.x;
@@ -525,10 +524,9 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
     const float bx0 = (float)wx0 * v.texel_x - 1.0f, bx1 = (float)(wx0 + 7) * v.texel_x - 1.0f;
     const float by0 = (float)wy0 * v.texel_y - 1.0f, by1 = (float)(wy0 + 7) * v.texel_y - 1.0f;
-    const f2 cyy = f2_pack(cy0, cy1);
     // pixels outside the image start done (T = 0)
     f2 TT = f2_pack(in0 ? 1.0f : 0.0f, in1 ? 1.0f : 0.0f);
-    f2 R = f2_dup(0.0f), G = f2_dup(0.0f), B = f2_dup(0.0f);
+    float R0 = 0.0f, R1 = 0.0f, G0 = 0.0f, G1 = 0.0f, B0 = 0.0f, B1 = 0.0f;
     const float tmin = a.t_min;
     const unsigned lt = lanemask_lt();
     bool done = !in0 && !in1;
@@ -551,28 +549,31 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
             const float4 q1 = __ldg(rp + 1);  // (A, B, C, L)
             const float4 q2 = __ldg(rp + 2);  // (red, green, blue, 0)
             s_s[warp][k] = make_float4(q0.x, q1.x, q1.y, q1.w);
-            s_yc[warp][k] = make_ulonglong2(f2_dup(q0.y), f2_dup(q1.z));
-            s_rg[warp][k] = make_ulonglong2(f2_dup(q2.x), f2_dup(q2.y));
-            s_bl[warp][k] = f2_dup(q2.z);
+            s_q[warp][k] = make_float4(q0.y, q1.z, q2.x, q2.y);
+            s_b[warp][k] = q2.z;
         }
         __syncwarp();  // slot writes visible to the whole warp
         const int cnt = __popc(bal);
 #pragma unroll 2
         for (int k = 0; k < cnt; ++k) {
             const float4 e = s_s[warp][k];
-            const ulonglong2 yc = s_yc[warp][k];
-            const ulonglong2 rg = s_rg[warp][k];
+            const float4 q = s_q[warp][k];
+            const float bl = s_b[warp][k];
             const float dx = cx - e.x;
-            const f2 adx2 = f2_dup(fmaf(e.y * dx, dx, e.w));  // A dx^2 + L
-            const f2 bdx = f2_dup(e.z * dx);
-            const f2 dyy = f2_sub(cyy, yc.x);
-            const f2 p = f2_fma(f2_fma(yc.y, dyy, bdx), dyy, adx2);
-            float p0, p1;
-            f2_unpack(p, p0, p1);
+            const float adx2 = fmaf(e.y * dx, dx, e.w);  // A dx^2 + L
+            const float bdx = __fmul_rn(e.z, dx);  // kept apart from the fma below
+            const float dy0 = cy0 - q.x, dy1 = cy1 - q.x;
+            const float p0 = fmaf(fmaf(q.y, dy0, bdx), dy0, adx2);
+            const float p1 = fmaf(fmaf(q.y, dy1, bdx), dy1, adx2);
             const f2 w = f2_mul(TT, f2_pack(ex2_approx(p0), ex2_approx(p1)));
-            R = f2_fma(rg.x, w, R);
-            G = f2_fma(rg.y, w, G);
-            B = f2_fma(s_bl[warp][k], w, B);
+            float w0, w1;
+            f2_unpack(w, w0, w1);
+            R0 = fmaf(q.z, w0, R0);
+            R1 = fmaf(q.z, w1, R1);
+            G0 = fmaf(q.w, w0, G0);
+            G1 = fmaf(q.w, w1, G1);
+            B0 = fmaf(bl, w0, B0);
+            B1 = fmaf(bl, w1, B1);
             TT = f2_sub(TT, w);
         }
         __syncwarp();  // slots are rewritten by the next chunk
@@ -580,12 +581,8 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
         f2_unpack(TT, T0, T1);
         done = T0 < tmin && T1 < tmin;
     }
-    float r0, r1, g0, g1, b0, b1;
-    f2_unpack(R, r0, r1);
-    f2_unpack(G, g0, g1);
-    f2_unpack(B, b0, b1);
-    if (in0) store_pixel(v, px, py0, r0, g0, b0);
-    if (in1) store_pixel(v, px, py1, r1, g1, b1);
+    if (in0) store_pixel(v, px, py0, R0, G0, B0);
+    if (in1) store_pixel(v, px, py1, R1, G1, B1);
 }
 
 template <int TW, int TH>
