@@ -235,66 +235,51 @@ __device__ __forceinline__ int slot_at(const RasterArgs& a, const uint64_t* sk, 
 // The reference's blend and termination, bit for bit: every pixel evaluates
 // every entry, in batches of 32, and after each batch the tile stops once no
 // pixel has T > 0.02.  Each warp owns an 8x8 pixel block, two pixels per
-// thread (rows y and y + 4, same column), blended as one packed f32x2 pair:
-// the pair shares dx and every per-splat operand, so one packed instruction
-// does the work of the two scalar ones with the same rounding.  The
-// reference's expression (gaussian_render.cu:727-737) as nvcc contracts it:
+// thread (rows y and y + 4, same column) that share dx and the column terms.
+// The reference's expression (gaussian_render.cu:727-737) as nvcc contracts it:
 //   q     = fma((2 b) dx, dy, fma(a dx, dx, (c dy) dy))
 //   alpha = opacity * sat(__expf(-0.5 q))
 //   rgb   = fma(rgb_s T, alpha, rgb);   T = T (1 - alpha)
-// Only __expf and the saturation run per pixel.  The batches are
-// double-buffered: the first warp starts asynchronous copies (cp.async,
-// global -> shared, no registers held) of batch k + 1 and loads the indices
-// of batch k + 2 before the tile blends batch k; once its own copies have
-// landed, each of its lanes rewrites its entry with every value duplicated
-// into both halves of a pair (the operand layout of the packed blend), and
-// the barrier that ends batch k publishes batch k + 1.
+// Every lane reads each entry from shared memory (40 bytes: centre, conic,
+// colour, as staged), so the tile's reads of an entry are as small as the
+// entry: the shared-memory data path, not the FP32 pipe, bounds this loop.
+// The batches are double-buffered: the first warp starts asynchronous
+// copies (cp.async, global -> shared, no registers held) of batch k + 1 and
+// loads the indices of batch k + 2 before the tile blends batch k; the
+// barrier that ends batch k publishes batch k + 1.
 struct RefSmem {
     float2 xy[64];
-    float4 con[64];
-    float4 col[64];
-    ulonglong2 dp[64];  // {x, x}, {y, y}
-    ulonglong2 dq[64];  // {a, a}, {c, c}
-    ulonglong2 dr[64];  // {2 b, 2 b}, {opacity, opacity}
-    ulonglong2 ds[64];  // {red, red}, {green, green}
-    f2 dbl[64];         // {blue, blue}
+    float4 con[64];  // (a, b, c, -)
+    float4 col[64];  // (red, green, blue, opacity)
 };
 
-// Rewrites staged entry `slot` as duplicated pairs.  2 b is exact (a power
-// of two scaling), so forming it here changes no rounding.
-__device__ __forceinline__ void dup_entry(RefSmem& sm, const int slot)
+// One pixel of the pair: dy, the row terms, alpha, colour and T.
+__device__ __forceinline__ void blend_ref_pixel(const float cy, const float y, const float dx, const float adx,
+                                                const float b2dx, const float4 k, const float4 col, float& R, float& G,
+                                                float& B, float& T)
 {
-    const float2 c = sm.xy[slot];
-    const float4 k = sm.con[slot];
-    const float4 col = sm.col[slot];
-    sm.dp[slot] = make_ulonglong2(f2_dup(c.x), f2_dup(c.y));
-    sm.dq[slot] = make_ulonglong2(f2_dup(k.x), f2_dup(k.z));
-    sm.dr[slot] = make_ulonglong2(f2_dup(2.0f * k.y), f2_dup(col.w));
-    sm.ds[slot] = make_ulonglong2(f2_dup(col.x), f2_dup(col.y));
-    sm.dbl[slot] = f2_dup(col.z);
+    const float dy = __fsub_rn(cy, y);
+    const float inner = fmaf(adx, dx, __fmul_rn(__fmul_rn(k.z, dy), dy));
+    const float q = fmaf(b2dx, dy, inner);
+    const float alpha = __fmul_rn(col.w, __saturatef(__expf(__fmul_rn(-0.5f, q))));
+    R = fmaf(__fmul_rn(col.x, T), alpha, R);
+    G = fmaf(__fmul_rn(col.y, T), alpha, G);
+    B = fmaf(__fmul_rn(col.z, T), alpha, B);
+    T = __fmul_rn(T, __fsub_rn(1.0f, alpha));
 }
 
-__device__ __forceinline__ void blend_ref_pair(const float cx, const f2 cyy, const RefSmem& sm, const int j, f2& R,
-                                               f2& G, f2& B, f2& TT)
+// 2 b is exact (a power of two scaling), so forming it here changes no rounding.
+__device__ __forceinline__ void blend_ref_pair(const float cx, const float cy0, const float cy1, const RefSmem& sm,
+                                               const int j, float (&R)[2], float (&G)[2], float (&B)[2], float (&T)[2])
 {
-    const ulonglong2 P = sm.dp[j], Q = sm.dq[j], S = sm.dr[j], C = sm.ds[j];
-    // the column terms are the same for both pixels: one scalar operation each
-    float sx, a, b2, unused;
-    f2_unpack(P.x, sx, unused);
-    f2_unpack(Q.x, a, unused);
-    f2_unpack(S.x, b2, unused);
-    const float dx = cx - sx;
-    const f2 dxx = f2_dup(dx);
-    const f2 dyy = f2_sub(cyy, P.y);
-    const f2 inner = f2_fma(f2_dup(a * dx), dxx, f2_mul(f2_mul(Q.y, dyy), dyy));
-    const f2 q = f2_fma(f2_dup(b2 * dx), dyy, inner);
-    float h0, h1;
-    f2_unpack(f2_mul(f2_dup(-0.5f), q), h0, h1);
-    const f2 alpha = f2_mul(S.y, f2_pack(__saturatef(__expf(h0)), __saturatef(__expf(h1))));
-    R = f2_fma(f2_mul(C.x, TT), alpha, R);
-    G = f2_fma(f2_mul(C.y, TT), alpha, G);
-    B = f2_fma(f2_mul(sm.dbl[j], TT), alpha, B);
-    TT = f2_mul(TT, f2_sub(f2_dup(1.0f), alpha));
+    const float2 c = sm.xy[j];
+    const float4 k = sm.con[j];
+    const float4 col = sm.col[j];
+    const float dx = __fsub_rn(cx, c.x);
+    const float adx = __fmul_rn(k.x, dx);
+    const float b2dx = __fmul_rn(2.0f * k.y, dx);
+    blend_ref_pixel(cy0, c.y, dx, adx, b2dx, k, col, R[0], G[0], B[0], T[0]);
+    blend_ref_pixel(cy1, c.y, dx, adx, b2dx, k, col, R[1], G[1], B[1], T[1]);
 }
 
 template <int TW, int TH>
@@ -325,8 +310,7 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy0 = (float)py0 * v.texel_y - 1.0f;
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
-    const f2 cyy = f2_pack(cy0, cy1);
-    f2 R = f2_dup(0.0f), G = f2_dup(0.0f), B = f2_dup(0.0f), TT = f2_dup(1.0f);
+    float R[2] = {0.0f, 0.0f}, G[2] = {0.0f, 0.0f}, B[2] = {0.0f, 0.0f}, T[2] = {1.0f, 1.0f};
     const RasterSmem rs = {sm.xy, sm.con, sm.col, nullptr};
     const bool loader = threadIdx.x < 32;
     const int t = (int)threadIdx.x;
@@ -334,7 +318,6 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
     cp_async_commit();
     int idx_next = (loader && 32 + t < count) ? slot_at(a, sk, first, 32 + t) : 0;
     cp_async_wait_all();
-    if (loader && t < count) dup_entry(sm, t);
     __syncthreads();
     for (int base = 0; base < count; base += 32) {
         const int buf = (base >> 5) & 1;
@@ -347,23 +330,16 @@ __device__ __forceinline__ void raster_ref_tile(const RasterArgs& a, const ViewP
         const int j0 = 32 * buf;
         if (nb == 32) {
 #pragma unroll 8
-            for (int j = j0; j < j0 + 32; ++j) blend_ref_pair(cx, cyy, sm, j, R, G, B, TT);
+            for (int j = j0; j < j0 + 32; ++j) blend_ref_pair(cx, cy0, cy1, sm, j, R, G, B, T);
         } else {
-            for (int j = j0; j < j0 + nb; ++j) blend_ref_pair(cx, cyy, sm, j, R, G, B, TT);
+            for (int j = j0; j < j0 + nb; ++j) blend_ref_pair(cx, cy0, cy1, sm, j, R, G, B, T);
         }
         idx_next = idx2;
         cp_async_wait_all();
-        if (more) dup_entry(sm, 32 * (buf ^ 1) + t);
-        float T0, T1;
-        f2_unpack(TT, T0, T1);
-        if (__syncthreads_count((in0 && T0 > 0.02f) || (in1 && T1 > 0.02f)) == 0) break;
+        if (__syncthreads_count((in0 && T[0] > 0.02f) || (in1 && T[1] > 0.02f)) == 0) break;
     }
-    float r0, r1, g0, g1, b0, b1;
-    f2_unpack(R, r0, r1);
-    f2_unpack(G, g0, g1);
-    f2_unpack(B, b0, b1);
-    if (in0) store_pixel(v, px, py0, r0, g0, b0);
-    if (in1) store_pixel(v, px, py1, r1, g1, b1);
+    if (in0) store_pixel(v, px, py0, R[0], G[0], B[0]);
+    if (in1) store_pixel(v, px, py1, R[1], G[1], B[1]);
 }
 
 template <int TW, int TH>
@@ -455,9 +431,12 @@ __global__ void __launch_bounds__(TW * TH) raster_persistent_kernel(RasterArgs a
 // tile's warps) and tests its cull extents against the block; the
 // survivors are packed in list order into per-warp shared-memory slots
 // (rank = popcount of the ballot below the lane) and every lane blends them
-// into both its pixels as one packed f32x2 pair.  The column terms of the
-// exponent (A dx^2 + L, B dx) are formed once per lane in scalar
-// arithmetic; the pair shares them.
+// into both its pixels.  Every lane reads every survivor, so the slots hold
+// each value once (36 bytes: x, A, B, L, y, C and the colour): the
+// shared-memory reads, not the arithmetic, bound this loop, and duplicated
+// pair operands would double them.  The column terms of the exponent
+// (A dx^2 + L, B dx) are formed once per lane and shared by its two pixels;
+// the weights and T are updated as one packed f32x2 pair.
 // Blend per pixel: alpha = 2^(A dx^2 + B dx dy + C dy^2 + L) (opacity
 // folded in as L = log2(opacity); the conics are positive definite, so
 // alpha <= opacity), w = T alpha, colour += rgb w, T -= w.  A warp stops
@@ -471,14 +450,6 @@ __device__ __forceinline__ float ex2_approx(const float x)
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
-
-// One survivor, as the pair reads it: scalar terms and duplicated pairs.
-struct RecSlot {
-    float4 s;       // (x, A, B, opacity)
-    ulonglong2 yc;  // {y, y}, {C, C}
-    ulonglong2 rg;  // {red, red}, {green, green}
-    f2 bl;          // {blue, blue}
-};
 
 template <int TW, int TH>
 __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kernel(RasterArgs a)
