@@ -502,23 +502,34 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
     const unsigned lt = lanemask_lt();
     bool done = !in0 && !in1;
 
+    // each chunk's cull records are loaded one chunk ahead, so their
+    // latency overlaps the blend of the chunk before
+    float4 qn = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4* rpn = nullptr;
+    if (first + lane < last) {
+        rpn = a.rec + 3 * (int64_t)slot_at(a, sk, first, lane);
+        qn = __ldg(rpn);
+    }
     for (int base = first; base < last; base += 32) {
         if (__all_sync(kFull, done)) break;
         const int j = base + lane;
         bool keep = false;
-        float4 q0;
-        const float4* rp = nullptr;
-        if (j < last) {
-            const int s = slot_at(a, sk, first, j - first);
-            rp = a.rec + 3 * (int64_t)s;
-            q0 = __ldg(rp);  // (x, y, ext_x, ext_y)
+        const float4 q0 = qn;  // (x, y, ext_x, ext_y)
+        const float4* rp = rpn;
+        if (j < last)
             keep = (q0.x - q0.z <= bx1) && (q0.x + q0.z >= bx0) && (q0.y - q0.w <= by1) && (q0.y + q0.w >= by0);
-        }
         const unsigned bal = __ballot_sync(kFull, keep);
+        float4 q1, q2;
+        if (keep) {
+            q1 = __ldg(rp + 1);  // (A, B, C, L)
+            q2 = __ldg(rp + 2);  // (red, green, blue, 0)
+        }
+        if (j + 32 < last) {
+            rpn = a.rec + 3 * (int64_t)slot_at(a, sk, first, j + 32 - first);
+            qn = __ldg(rpn);
+        }
         if (keep) {
             const int k = __popc(bal & lt);
-            const float4 q1 = __ldg(rp + 1);  // (A, B, C, L)
-            const float4 q2 = __ldg(rp + 2);  // (red, green, blue, 0)
             s_s[warp][k] = make_float4(q0.x, q1.x, q1.y, q1.w);
             s_q[warp][k] = make_float4(q0.y, q1.z, q2.x, q2.y);
             s_b[warp][k] = q2.z;
