@@ -536,7 +536,7 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
         }
         __syncwarp();  // slot writes visible to the whole warp
         const int cnt = __popc(bal);
-#pragma unroll 2
+#pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
             const float4 e = s_s[warp][k];
             const float4 q = s_q[warp][k];
