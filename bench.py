@@ -36,7 +36,7 @@ N_GAUSS = 3_000_000
 # rendered alone: ncu capture of the second frame of `bench.py --views 1
 # --steps 1 --warmup 1 --no-cpu --no-e2e --no-plain --no-serve` (128.2 MB
 # read, 7.0 MB written; the raster roofline's traffic)
-RASTER_VIEW0_TRAFFIC = 135.2e6
+RASTER_VIEW0_TRAFFIC = 133.7e6
 RING_RADIUS = 15.0
 WORKLOAD = "3M Gaussians SH3, 64-view orbit ring r=15, 1280x720/1600x900/1920x1080 cycling, one batched frame"
 
