@@ -146,6 +146,7 @@ _sig("gs_autotune", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(
      ctypes.POINTER(_I32), _P)
 _sig("gs_autotune_lookup", _I, _P, _I64, _I32, _I32, _I32, ctypes.POINTER(gs_render_cfg), ctypes.POINTER(_I32))
 _sig("gs_autotune_entries", _I32, _P)
+_sig("gs_autotune_bucket", _I, _I64, _I32, _I32, _I32, ctypes.POINTER(_I32))
 _sig("gs_stage_sh", _I, _I64, _P, _P, _I32, _I32, ctypes.POINTER(gs_camera), _P, _P)
 _sig("gs_stage_project", _I, _I64, _P, _P, ctypes.POINTER(gs_camera), _P, _P, _P, _P, _P)
 _sig("gs_stage_build", _I, _P, _I64, _P, _P, _P, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P, _P,
@@ -421,6 +422,14 @@ def autotune(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig, iteratio
     check(lib.gs_autotune(ctx.h, scene.h, arr, len(cams), ctypes.byref(c), iterations, ctypes.byref(best),
                           ctypes.byref(best_ms), res, 64, ctypes.byref(count), _stream_ptr(stream)), "gs_autotune")
     return _from_c(best), best_ms.value, [(_from_c(r.cfg), r.ms) for r in res[:min(count.value, 64)]]
+
+
+def autotune_bucket(n: int, width: int, height: int, num_views: int) -> tuple:
+    """(floor log2 N, floor log2 pixels, view-count class) of a batch: the
+    key of the tuning table."""
+    b = (_I32 * 3)()
+    check(lib.gs_autotune_bucket(n, width, height, num_views, b), "gs_autotune_bucket")
+    return tuple(b)
 
 
 def autotune_lookup(ctx: Context, n: int, width: int, height: int, num_views: int, cfg: RenderConfig):

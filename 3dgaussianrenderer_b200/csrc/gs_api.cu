@@ -1718,6 +1718,15 @@ int gs_autotune_lookup(gs_ctx* ctx, int64_t n, int32_t width, int32_t height, in
     return GS_OK;
 }
 
+int gs_autotune_bucket(int64_t n, int32_t width, int32_t height, int32_t num_views, int32_t bucket[3])
+{
+    if (!bucket || n < 0 || width <= 0 || height <= 0 || num_views <= 0) return fail(GS_ERR_INVALID, "bad bucket");
+    bucket[0] = floor_log2(n);
+    bucket[1] = floor_log2((int64_t)width * height);
+    bucket[2] = views_bucket(num_views);
+    return GS_OK;
+}
+
 int32_t gs_autotune_entries(gs_ctx* ctx)
 {
     if (!ctx) return 0;

@@ -212,6 +212,11 @@ GS_API int gs_autotune_lookup(gs_ctx* ctx, int64_t n, int32_t width, int32_t hei
                               gs_render_cfg* cfg, int32_t* found);
 /* Entries in the context's tuning table. */
 GS_API int32_t gs_autotune_entries(gs_ctx* ctx);
+/* The bucket gs_autotune and gs_autotune_lookup file a batch under:
+ * bucket[0] = floor(log2 n) (-1 for n = 0), bucket[1] = floor(log2(width *
+ * height)), bucket[2] = view-count class 0..5 (1, 2-4, 5-8, 9-16, 17-32,
+ * 33+).  No device work. */
+GS_API int gs_autotune_bucket(int64_t n, int32_t width, int32_t height, int32_t num_views, int32_t bucket[3]);
 
 /* ---- performance overlay (app/perf_overlay.cpp:115-161) ---------------- */
 

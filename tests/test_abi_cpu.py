@@ -133,3 +133,17 @@ def test_image_writers_flip_rows_and_round_trip(gs, tmp_path):
     assert np.array_equal(raw[:, 1:].reshape(300, 200, 4), big[::-1])
     with pytest.raises(gs.GsError):
         gs.write_image(str(tmp_path / "no_such_dir" / "x.png"), img)
+
+
+def test_autotune_buckets(gs):
+    """The tuning table's key, computed on the host: powers of two of N and
+    of the pixel count, and six view-count classes."""
+    assert gs.autotune_bucket(3_000_000, 1920, 1080, 64) == (21, 20, 5)
+    assert gs.autotune_bucket((1 << 20) - 1, 1024, 1024, 1) == (19, 20, 0)
+    assert gs.autotune_bucket(1 << 20, 1024, 1023, 1) == (20, 19, 0)
+    assert gs.autotune_bucket(0, 1, 1, 1) == (-1, 0, 0)
+    classes = [gs.autotune_bucket(1000, 64, 64, v)[2] for v in (1, 2, 4, 5, 8, 9, 16, 17, 32, 33, 1000)]
+    assert classes == [0, 1, 1, 2, 2, 3, 3, 4, 4, 5, 5]
+    for bad in ((-1, 64, 64, 1), (10, 0, 64, 1), (10, 64, 64, 0)):
+        with pytest.raises(gs.GsError):
+            gs.autotune_bucket(*bad)
