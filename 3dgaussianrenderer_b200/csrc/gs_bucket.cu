@@ -263,7 +263,9 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
                 if (has) {
                     const int c = __ffs(m) - 1;
                     m &= m - 1;
-                    gt = toff + (int64_t)(r.y + c / r.z) * tiles_x + (r.x + c % r.z);
+                    int cy, cx;
+                    divmod_small(c, r.z, cy, cx);
+                    gt = toff + (int64_t)(r.y + cy) * tiles_x + (r.x + cx);
                 }
                 put_keys(a, has, gt, depth, slot);
             }
@@ -280,7 +282,9 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
                     if (m) {
                         const int c = __ffs(m) - 1;
                         m &= m - 1;
-                        gt[u] = toff + (int64_t)(r.y + c / r.z) * tiles_x + (r.x + c % r.z);
+                        int cy, cx;
+                        divmod_small(c, r.z, cy, cx);
+                        gt[u] = toff + (int64_t)(r.y + cy) * tiles_x + (r.x + cx);
                     }
                 }
 #pragma unroll

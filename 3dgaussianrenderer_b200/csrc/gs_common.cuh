@@ -541,12 +541,39 @@ __device__ __forceinline__ int4 tile_rect(const Ell& e, const ViewParams& v)
 
 __device__ __forceinline__ int rect_candidates(const int4 r) { return imax(0, r.z * r.w); }
 
+// C's quotient and remainder of c / d for c >= 0.  For d >= 1 and
+// c < 2^20 a float estimate (the hardware reciprocal is within a few ulp, so
+// the estimate is within 1 of the quotient) and one correction step either
+// way: exact, and shorter than the integer division sequence.  Larger c,
+// and d <= 0 (the inverted rectangles of NaN axes), take the integer
+// division.
+__device__ __forceinline__ void divmod_small(const int c, const int d, int& q, int& r)
+{
+    if (d <= 0 || c >= (1 << 20)) {
+        q = c / d;
+        r = c % d;
+        return;
+    }
+    int qq = (int)(__int2float_rn(c) * rcp_approx(__int2float_rn(d)));
+    int rr = c - qq * d;
+    if (rr < 0) {
+        --qq;
+        rr += d;
+    } else if (rr >= d) {
+        ++qq;
+        rr -= d;
+    }
+    q = qq;
+    r = rr;
+}
+
 // Candidate c of a tile rectangle, row-major (gaussian_render.cu:466-483).
 // Returns true on overlap and the view-local tile index.
 template <bool FAST = false>
 __device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const int c, const ViewParams& v, int& tile)
 {
-    const int lx = c % r.z, ly = c / r.z;
+    int lx, ly;
+    divmod_small(c, r.z, ly, lx);
     const int gx = r.x + lx, gy = r.y + ly;
     const float tx0 = (float)gx * v.tclip_x - 1.0f;
     const float ty0 = (float)gy * v.tclip_y - 1.0f;

@@ -424,7 +424,9 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
                 while (m) {
                     const int c = __ffs(m) - 1;
                     m &= m - 1;
-                    const int gx = r.x + c % r.z, gy = r.y + c / r.z;
+                    int ly, lx;
+                    divmod_small(c, r.z, ly, lx);
+                    const int gx = r.x + lx, gy = r.y + ly;
                     if (dst < a.capacity) {
                         a.keys[dst] = make_key((uint64_t)(v.tile_offset + gy * v.tiles_x + gx), depth);
                         a.values[dst] = (int32_t)gi;
