@@ -89,3 +89,23 @@ def test_stress_batch_views_identical_to_single(stress):
     assert total == st["num_keys"]
     scene.close()
     ctx.close()
+
+
+def test_stress_large_host_batch_renders_in_parts(stress):
+    """A host-output batch of more than 16 views whose tile lists exceed
+    2^31 entries: the grouped one-frame path gives way to frames over parts
+    of the views, and the images are those of the views rendered alone."""
+    gs, sc, sh, cams = stress
+    ctx = gs.Context(0)
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], sh, 3)
+    rc = gs.RenderConfig()
+    views = [cams[v % VIEWS] for v in range(18)]
+    size = W * H * 4
+    out = np.zeros(len(views) * size, np.uint8)
+    st = gs.render_batch_host(ctx, scene, views, rc, out)
+    assert st["num_keys"] >= 1 << 31
+    for v in (0, 9, 17):
+        single, _ = gs.render_host(ctx, scene, views[v], rc)
+        assert np.array_equal(out[v * size:(v + 1) * size].reshape(single.shape), single), v
+    scene.close()
+    ctx.close()
