@@ -36,6 +36,7 @@ GS_ERR_CAPACITY = 3
 GS_ERR_DEVICE_TIMEOUT = 4
 GS_ERR_CUDA = 5
 GS_ERR_NO_DEVICE = 6
+GS_ERR_CANCELLED = 7
 GS_TERM_REFERENCE = 0
 GS_TERM_TMIN = 1
 GS_ORDER_BUCKETS = 0
@@ -100,6 +101,11 @@ class gs_tune_result(ctypes.Structure):
     _fields_ = [("cfg", gs_render_cfg), ("ms", ctypes.c_double)]
 
 
+class gs_frame_probe(ctypes.Structure):
+    _fields_ = [("d_xy", ctypes.c_void_p), ("d_z", ctypes.c_void_p), ("d_ellipse", ctypes.c_void_p),
+                ("d_conic", ctypes.c_void_p), ("d_color", ctypes.c_void_p)]
+
+
 _P = ctypes.c_void_p
 _I = ctypes.c_int
 _I32 = ctypes.c_int32
@@ -154,6 +160,12 @@ _sig("gs_stage_build", _I, _P, _I64, _P, _P, _P, ctypes.POINTER(gs_camera), ctyp
 _sig("gs_stage_sort", _I, _P, _I64, _I32, _P, _P, _P, _P, ctypes.POINTER(_I32), _P)
 _sig("gs_stage_ranges", _I, _I64, _P, _I64, _P, _P)
 _sig("gs_stage_raster", _I, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P, _P, _P, _P, _P, _P, _P)
+_sig("gs_probe_frame", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(gs_render_cfg), ctypes.POINTER(_P),
+     ctypes.POINTER(gs_frame_probe), ctypes.POINTER(gs_stats), _P)
+_sig("gs_probe_tile_lists", _I, _P, _P, _I64, _P, _P, _I64, _P, _I64, ctypes.POINTER(_I64), ctypes.POINTER(_I32))
+_sig("gs_test_fail_allocations", None, _I32, _I32)
+_sig("gs_test_pending_allocation_failures", _I32)
+_sig("gs_test_bounded_wait", _I, _I32, _P)
 _sig("gs_num_tiles", _I64, _I32, _I32, ctypes.POINTER(gs_render_cfg))
 _sig("gs_key_bits", _I32, _I64)
 
@@ -403,6 +415,41 @@ def render_batch_host(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig,
     return st.as_dict()
 
 
+def probe_frame(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig, outs: list, xy, z, ell, conic,
+                color=None, stream=None) -> dict:
+    """A tile-bucket frame (as render_batch, never a graph replay) that also
+    writes, per (view, Gaussian) at view * n + caller index, the projected
+    centre, depth, ellipse and conic (and the colour of the Gaussians that
+    reach a tile) into the given device tensors."""
+    arr = (gs_camera * len(cams))(*[c.c for c in cams])
+    ptrs = (_P * len(outs))(*[_ptr(o) for o in outs])
+    pr = gs_frame_probe(_ptr(xy), _ptr(z), _ptr(ell), _ptr(conic), _ptr(color))
+    st = gs_stats()
+    c = cfg.c()
+    check(lib.gs_probe_frame(ctx.h, scene.h, arr, len(cams), ctypes.byref(c), ptrs, ctypes.byref(pr),
+                             ctypes.byref(st), _stream_ptr(stream)), "gs_probe_frame")
+    return st.as_dict()
+
+
+def probe_tile_lists(ctx: Context) -> dict:
+    """Tile lists of the context's last tile-bucket frame: ranges (T, 2),
+    keys as emitted (depth << 32 | slot), order (slots in blend order of the
+    tiles larger than fused_cap), slot_index (view * n + caller index)."""
+    sizes = (_I64 * 3)()
+    cap = _I32()
+    check(lib.gs_probe_tile_lists(ctx.h, None, 0, None, None, 0, None, 0, sizes, ctypes.byref(cap)),
+          "gs_probe_tile_lists")
+    T, K, S = (int(x) for x in sizes)
+    ranges = np.zeros(2 * max(T, 1), np.int32)
+    keys = np.zeros(max(K, 1), np.uint64)
+    order = np.zeros(max(K, 1), np.int32)
+    slots = np.zeros(max(S, 1), np.int32)
+    check(lib.gs_probe_tile_lists(ctx.h, _ptr(ranges), ranges.size, _ptr(keys), _ptr(order), keys.size, _ptr(slots),
+                                  slots.size, sizes, ctypes.byref(cap)), "gs_probe_tile_lists")
+    return {"ranges": ranges[:2 * T].reshape(T, 2), "keys": keys[:K], "order": order[:K], "slot_index": slots[:S],
+            "fused_cap": cap.value}
+
+
 def _from_c(c: gs_render_cfg) -> "RenderConfig":
     return RenderConfig(c.sh_max_degree, c.termination, c.t_min, c.tile_w, c.tile_h, c.ordering, c.sort_variant,
                         c.views_per_block, c.graph)
@@ -564,6 +611,8 @@ _sig("gs_server_submit", _I, _P, _I32, ctypes.POINTER(gs_camera), _P, ctypes.POI
 _sig("gs_server_wait", _I, _P, _I64, ctypes.c_double, ctypes.POINTER(ctypes.c_double))
 _sig("gs_server_get_stats", _I, _P, ctypes.POINTER(gs_server_stats))
 _sig("gs_server_reset_stats", _I, _P)
+_sig("gs_server_cancel", _I, _P, _I64)
+_sig("gs_server_pause", _I, _P, _I32)
 _sig("gs_ply_info", _I, ctypes.c_char_p, ctypes.POINTER(_I64), ctypes.POINTER(_I32))
 _sig("gs_ply_last_error", ctypes.c_char_p)
 _sig("gs_ply_read", _I, ctypes.c_char_p, _P, _P, _P, _P, _P)
@@ -620,6 +669,20 @@ class Server:
         lat = ctypes.c_double(0)
         check(lib.gs_server_wait(self.h, rid, timeout_ms, ctypes.byref(lat)), "gs_server_wait")
         return float(lat.value)
+
+    def wait_status(self, rid: int, timeout_ms: float = 60_000.0) -> int:
+        """The request's completion status (GS_OK, GS_ERR_CANCELLED, ...)
+        without raising."""
+        lat = ctypes.c_double(0)
+        return int(lib.gs_server_wait(self.h, rid, timeout_ms, ctypes.byref(lat)))
+
+    def cancel(self, rid: int) -> int:
+        """Cancels a queued request; GS_ERR_INVALID when it is already on the
+        device, finished or unknown."""
+        return int(lib.gs_server_cancel(self.h, rid))
+
+    def pause(self, paused: bool = True):
+        check(lib.gs_server_pause(self.h, 1 if paused else 0), "gs_server_pause")
 
     def stats(self) -> dict:
         s = gs_server_stats()

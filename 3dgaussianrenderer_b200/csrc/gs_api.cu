@@ -48,6 +48,29 @@ int cuda_fail(cudaError_t e, const char* where)
         if (_e != cudaSuccess) return cuda_fail(_e, #call);      \
     } while (0)
 
+// Test hook (gs_test_fail_allocations): after g_alloc_skip more buffer
+// allocations, the next g_fail_allocs fail as if the device were out of
+// memory.
+std::mutex g_alloc_hook_mu;
+int g_alloc_skip = 0, g_fail_allocs = 0;
+std::atomic<bool> g_alloc_hook{false};
+
+bool injected_alloc_failure()
+{
+    if (!g_alloc_hook.load(std::memory_order_relaxed)) return false;
+    std::lock_guard<std::mutex> lk(g_alloc_hook_mu);
+    if (g_alloc_skip > 0) {
+        --g_alloc_skip;
+        return false;
+    }
+    if (g_fail_allocs > 0) {
+        if (--g_fail_allocs == 0) g_alloc_hook = false;
+        return true;
+    }
+    g_alloc_hook = false;
+    return false;
+}
+
 struct DevBuf {
     void* p = nullptr;
     size_t bytes = 0;
@@ -58,6 +81,7 @@ struct DevBuf {
         if (p) cudaFree(p);
         p = nullptr;
         bytes = 0;
+        if (injected_alloc_failure()) return cudaErrorMemoryAllocation;
         const size_t sz = std::max<size_t>(need + need / 4, 256);
         cudaError_t e = cudaMalloc(&p, sz);
         if (e != cudaSuccess) {
@@ -145,6 +169,20 @@ constexpr size_t kMaxTuneEntries = 256;
 
 std::atomic<uint64_t> g_scene_uid{1};
 
+// Failure-path self-test (gs_test_bounded_wait): a decoupled look-back
+// from block 1 whose predecessor never publishes.  The wait gives up after
+// `spin_limit` polls, sets the error word and returns, as every look-back of
+// the pipeline does when a block it waits on never arrives.
+struct WaitWords {
+    uint64_t status[2];  // status[0] stays unpublished
+    int err;
+};
+
+__global__ void wait_selftest_kernel(WaitWords* w, int spin_limit)
+{
+    if (threadIdx.x == 0) look_back(w->status, 1, 1, 1u, &w->err, kErrTimeout, spin_limit);
+}
+
 // Internal status of a frame whose tile lists need 2^31 entries or more
 // (list positions are int32): run_frame renders it again as two frames
 // over halves of its views.
@@ -194,6 +232,10 @@ struct gs_ctx {
     uint64_t use_clock = 0;
     std::vector<TuneEntry> tune;           // gs_autotune's table
     uint64_t tune_clock = 0;
+    // the last tile-bucket frame (gs_probe_tile_lists); last_tiles < 0: none
+    // since the lists last changed
+    int64_t last_tiles = -1, last_keys = 0, last_slots = 0;
+    int32_t last_fused_cap = 0;
 };
 
 namespace {
@@ -305,8 +347,10 @@ int ensure_key_buffers(gs_ctx* ctx, int64_t keys)
 {
     if (keys <= ctx->key_capacity && ctx->keys0.p) return GS_OK;
     const size_t k = (size_t)std::max<int64_t>(keys, 1);
-    if (ctx->keys0.ensure(8 * k) || ctx->keys1.ensure(8 * k) || ctx->vals0.ensure(4 * k) || ctx->vals1.ensure(4 * k))
+    if (ctx->keys0.ensure(8 * k) || ctx->keys1.ensure(8 * k) || ctx->vals0.ensure(4 * k) || ctx->vals1.ensure(4 * k)) {
+        ctx->key_capacity = 0;  // some lists were released: regrow them all next time
         return fail(GS_ERR_OOM, "tile lists");
+    }
     const int64_t cap = std::min(std::min((int64_t)(ctx->keys0.bytes / 8), (int64_t)(ctx->keys1.bytes / 8)),
                                  std::min((int64_t)(ctx->vals0.bytes / 4), (int64_t)(ctx->vals1.bytes / 4)));
     ctx->key_capacity = std::min<int64_t>(cap, (1ll << 31) - 1);
@@ -352,8 +396,10 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
         const size_t m = (size_t)items;
         if (ctx->color.ensure(16 * m) || ctx->xy.ensure(8 * m) || ctx->z.ensure(4 * m) || ctx->ell.ensure(16 * m) ||
             ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(4 * m) ||
-            ctx->rec.ensure(48 * m) || ctx->hitmask.ensure(4 * m))
+            ctx->rec.ensure(48 * m) || ctx->hitmask.ensure(4 * m)) {
+            ctx->per_view_capacity = 0;  // some of them were released: re-check them all next time
             return fail(GS_ERR_OOM, "splat buffers");
+        }
         ctx->per_view_capacity = items;
     }
     if (sizeof(uint64_t) * (size_t)std::max<int64_t>(chains, 1) > ctx->scan_status.bytes) {
@@ -416,6 +462,7 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     if (K >= (1ll << 31)) return fail(kSplitViews, "more than 2^31 tile keys");
 
     // 2. emit keys
+    ctx->last_tiles = -1;  // the bucket frame's lists are overwritten from here on
     if (K > ctx->key_capacity) {
         rc = ensure_key_buffers(ctx, K);
         if (rc) return rc;
@@ -425,7 +472,6 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     GS_CUDA(cudaEventRecord(ctx->ev[2], st));
     EmitArgs ea{};
     ea.n = n;
-    ea.fast = cfg.termination == GS_TERM_TMIN;  // the frame kernel's arithmetic
     ea.num_views = num_views;
     ea.views = ctx->views.as<ViewParams>();
     ea.offsets = ctx->offsets.as<int32_t>();
@@ -511,6 +557,7 @@ struct FramePlan {
     int64_t n = 0, groups = 0, blocks = 0, items = 0, tiles_total = 0;
     int vpb = 0, deg = 0;
     const HostCopy* host_copy = nullptr;  // non-null: raster per view group, each group's end marked
+    const gs_frame_probe* probe = nullptr;  // non-null: the frame kernel also writes the probe outputs
 };
 
 // Validates the frame, fills the pinned view parameters and makes the
@@ -550,8 +597,10 @@ int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams,
         const size_t m = (size_t)p.items;
         if (ctx->color.ensure(16 * m) || ctx->xy.ensure(8 * m) || ctx->z.ensure(4 * m) || ctx->ell.ensure(16 * m) ||
             ctx->conic.ensure(16 * m) || ctx->rect.ensure(8 * m) || ctx->offsets.ensure(4 * m) ||
-            ctx->rec.ensure(48 * m) || ctx->hitmask.ensure(4 * m))
+            ctx->rec.ensure(48 * m) || ctx->hitmask.ensure(4 * m)) {
+            ctx->per_view_capacity = 0;  // some of them were released: re-check them all next time
             return fail(GS_ERR_OOM, "splat buffers");
+        }
         ctx->per_view_capacity = p.items;
     }
     const size_t tiles = (size_t)std::max<int64_t>(p.tiles_total, 1);
@@ -613,6 +662,13 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     fa.tile_count = ctx->tile_count.as<uint32_t>();
     fa.slot_counter = &dc->slots;
     fa.aggregate = p.tiles_total <= kAggregateMaxTiles;
+    if (p.probe) {
+        fa.probe_xy = reinterpret_cast<float2*>(p.probe->d_xy);
+        fa.probe_z = p.probe->d_z;
+        fa.probe_ell = reinterpret_cast<float4*>(p.probe->d_ellipse);
+        fa.probe_conic = reinterpret_cast<float4*>(p.probe->d_conic);
+        fa.probe_color = reinterpret_cast<float4*>(p.probe->d_color);
+    }
     if (p.n > 0) launch_frame_project(fa, p.deg, st, true);
 
     TileScanArgs ta{};
@@ -640,7 +696,6 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     BucketEmitArgs ea{};
     ea.n = p.n;
     ea.aggregate = p.tiles_total <= kAggregateMaxTiles;
-    ea.fast = cfg.termination == GS_TERM_TMIN;  // the frame kernel's arithmetic
     ea.slot_count = &dc->slots;
     ea.max_slots = p.items;
     ea.views = ctx->views.as<ViewParams>();
@@ -777,14 +832,16 @@ bool capture_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg& cfg,
 // With cfg.graph, the second frame with the same scene, options, view sizes
 // and outputs is captured into a CUDA graph and later ones replay it.
 int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
-                     uint8_t* const* outs, gs_stats* stats, cudaStream_t st, const HostCopy* hc = nullptr)
+                     uint8_t* const* outs, gs_stats* stats, cudaStream_t st, const HostCopy* hc = nullptr,
+                     const gs_frame_probe* probe = nullptr)
 {
     FramePlan p;
     int rc = plan_bucket_frame(ctx, scene, cams, num_views, cfg, outs, p);
     if (rc) return rc;
     p.host_copy = hc;
+    p.probe = probe;
     const int raster_groups = hc ? hc->groups : 0;
-    if (!ctx->keys0.p) {
+    if (!ctx->keys0.p || ctx->key_capacity == 0) {
         rc = ensure_key_buffers(ctx, std::max<int64_t>(p.items, 1 << 20));
         if (rc) return rc;
     }
@@ -868,6 +925,10 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         if (rc) return rc;
     }
 
+    ctx->last_tiles = p.tiles_total;
+    ctx->last_keys = ctx->h_counters->total;
+    ctx->last_slots = (int64_t)ctx->h_counters->slots;
+    ctx->last_fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     if (stats) {
         stats->sh_eval_ms = 0.0;
         stats->project_ms = ms_between(ctx->ev[0], ctx->ev[1]);
@@ -1026,6 +1087,7 @@ const char* gs_status_string(int status)
         case GS_ERR_DEVICE_TIMEOUT: return "bounded device wait timed out";
         case GS_ERR_CUDA: return "CUDA error";
         case GS_ERR_NO_DEVICE: return "no usable sm_100 device";
+        case GS_ERR_CANCELLED: return "request cancelled";
         default: return "unknown status";
     }
 }
@@ -1492,6 +1554,7 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     if (ctx->rect.ensure(8 * (size_t)n) || ctx->offsets.ensure(4 * (size_t)n) || ctx->hitmask.ensure(4 * (size_t)n))
         return fail(GS_ERR_OOM, "build buffers");
     ctx->per_view_capacity = 0;  // rect/offsets may have been regrown: force the frame path to re-check
+    ctx->last_tiles = -1;        // the last frame's slot indices are overwritten
     if (sizeof(uint64_t) * (size_t)blocks > ctx->scan_status.bytes) {
         if (ctx->scan_status.ensure(sizeof(uint64_t) * (size_t)blocks, true)) return fail(GS_ERR_OOM, "scan status");
     }
@@ -1526,9 +1589,9 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "build look-back timed out");
     const int64_t K = ctx->h_counters->total;
     *out_num_keys = K;
-    if (K > capacity) return fail(GS_ERR_CAPACITY, "tile list capacity exceeded");
     if (K > 0 && (!d_keys || !d_values)) return fail(GS_ERR_INVALID, "null key buffers");
-    EmitArgs ea{};  // exact candidate tests (the stage API's projection is exact)
+    if (capacity < 0) capacity = 0;
+    EmitArgs ea{};
     ea.n = n;
     ea.num_views = 1;
     ea.views = ctx->views.as<ViewParams>();
@@ -1543,8 +1606,12 @@ int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, 
     ea.keys = d_keys;
     ea.values = d_values;
     ea.capacity = capacity;
-    if (K > 0) launch_emit(ea, st);
+    if (K > 0 && capacity > 0) launch_emit(ea, st);
     GS_CUDA(cudaGetLastError());
+    // the reference truncates a list that does not fit and reports it full
+    // (gaussian_render.cu:506-509); here the first `capacity` keys in
+    // Gaussian order are written and the caller learns the exact count
+    if (K > capacity) return fail(GS_ERR_CAPACITY, "tile list capacity exceeded: the first `capacity` keys were written");
     return GS_OK;
 }
 
@@ -1611,7 +1678,7 @@ int gs_stage_raster(const gs_camera* cam, const gs_render_cfg* cfg, const int32_
     ra.conic = (const float4*)d_conic;
     ra.color = (const float4*)d_color;
     ra.t_min = cfg->t_min;
-    launch_raster(ra, cfg->tile_w, cfg->tile_h, cfg->termination, false, 148, (cudaStream_t)stream);
+    launch_raster(ra, cfg->tile_w, cfg->tile_h, cfg->termination, false, device_sm_count(), (cudaStream_t)stream);
     GS_CUDA(cudaGetLastError());
     return GS_OK;
 }
@@ -1745,6 +1812,93 @@ int32_t gs_key_bits(int64_t num_tiles)
     int32_t bits = 0;
     while (bits < 31 && (1ll << bits) < num_tiles) ++bits;
     return 32 + bits;
+}
+
+// ---- failure-path test hooks ------------------------------------------------------
+
+void gs_test_fail_allocations(int32_t skip, int32_t count)
+{
+    std::lock_guard<std::mutex> lk(g_alloc_hook_mu);
+    g_alloc_skip = skip > 0 ? skip : 0;
+    g_fail_allocs = count > 0 ? count : 0;
+    g_alloc_hook = g_fail_allocs > 0;
+}
+
+int32_t gs_test_pending_allocation_failures(void)
+{
+    std::lock_guard<std::mutex> lk(g_alloc_hook_mu);
+    return g_alloc_hook ? g_fail_allocs : 0;
+}
+
+int gs_test_bounded_wait(int32_t spin_limit, void* stream)
+{
+    if (spin_limit < 1 || spin_limit > kSpinLimit) return fail(GS_ERR_INVALID, "spin limit out of range");
+    cudaStream_t st = (cudaStream_t)stream;
+    WaitWords* w = nullptr;
+    GS_CUDA(cudaMalloc(&w, sizeof(WaitWords)));
+    int err = 0;
+    cudaError_t e = cudaMemsetAsync(w, 0, sizeof(WaitWords), st);
+    if (e == cudaSuccess) {
+        wait_selftest_kernel<<<1, 32, 0, st>>>(w, spin_limit);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&err, &w->err, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(w);
+    if (e != cudaSuccess) return cuda_fail(e, "bounded wait");
+    if (err == kErrTimeout) return fail(GS_ERR_DEVICE_TIMEOUT, "the bounded wait gave up, as it must");
+    return fail(GS_ERR_CUDA, "the bounded wait did not report its timeout");
+}
+
+// ---- frame probe ------------------------------------------------------------------
+
+int gs_probe_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                   const gs_render_cfg* cfg, uint8_t* const* d_rgba, const gs_frame_probe* probe, gs_stats* stats,
+                   void* stream)
+{
+    if (!ctx || !scene || !cams || !cfg || !d_rgba || !probe || num_views <= 0) return fail(GS_ERR_INVALID, "null argument");
+    if (!probe->d_xy || !probe->d_z || !probe->d_ellipse || !probe->d_conic)
+        return fail(GS_ERR_INVALID, "probe geometry outputs are required");
+    if (cfg->ordering != GS_ORDER_BUCKETS) return fail(GS_ERR_INVALID, "the probe covers GS_ORDER_BUCKETS frames");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    gs_render_cfg c = *cfg;
+    c.graph = 0;  // the probe outputs are arguments of this launch only
+    ctx->last_tiles = -1;
+    const int rc = run_frame_bucket(ctx, scene, cams, num_views, c, d_rgba, stats, (cudaStream_t)stream, nullptr, probe);
+    if (rc == kSplitViews) return fail(GS_ERR_CAPACITY, "the probe frame needs 2^31 tile keys or more");
+    return rc;
+}
+
+int gs_probe_tile_lists(gs_ctx* ctx, int32_t* h_ranges, int64_t ranges_capacity, uint64_t* h_keys, int32_t* h_order,
+                        int64_t keys_capacity, int32_t* h_slot_index, int64_t slots_capacity, int64_t out_sizes[3],
+                        int32_t* out_fused_cap)
+{
+    if (!ctx || !out_sizes) return fail(GS_ERR_INVALID, "null argument");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    if (ctx->last_tiles < 0) return fail(GS_ERR_INVALID, "no tile-bucket frame since the lists last changed");
+    out_sizes[0] = ctx->last_tiles;
+    out_sizes[1] = ctx->last_keys;
+    out_sizes[2] = ctx->last_slots;
+    if (out_fused_cap) *out_fused_cap = ctx->last_fused_cap;
+    GS_CUDA(cudaSetDevice(ctx->device));
+    if (h_ranges) {
+        if (ranges_capacity < 2 * ctx->last_tiles) return fail(GS_ERR_CAPACITY, "ranges buffer too small");
+        GS_CUDA(cudaMemcpy(h_ranges, ctx->ranges.p, sizeof(int32_t) * 2 * (size_t)ctx->last_tiles,
+                           cudaMemcpyDeviceToHost));
+    }
+    if (h_keys || h_order) {
+        if (keys_capacity < ctx->last_keys) return fail(GS_ERR_CAPACITY, "key buffers too small");
+        if (h_keys)
+            GS_CUDA(cudaMemcpy(h_keys, ctx->keys0.p, sizeof(uint64_t) * (size_t)ctx->last_keys, cudaMemcpyDeviceToHost));
+        if (h_order)
+            GS_CUDA(cudaMemcpy(h_order, ctx->vals0.p, sizeof(int32_t) * (size_t)ctx->last_keys, cudaMemcpyDeviceToHost));
+    }
+    if (h_slot_index) {
+        if (slots_capacity < ctx->last_slots) return fail(GS_ERR_CAPACITY, "slot buffer too small");
+        GS_CUDA(cudaMemcpy(h_slot_index, ctx->offsets.p, sizeof(int32_t) * (size_t)ctx->last_slots,
+                           cudaMemcpyDeviceToHost));
+    }
+    return GS_OK;
 }
 
 }  // extern "C"

@@ -333,8 +333,7 @@ __global__ void __launch_bounds__(kThreads) emit_bucket_kernel(BucketEmitArgs a)
             if (c < total) {
                 int tile = 0;
                 const ViewParams& v = a.views[oview];
-                hit = a.fast ? candidate_hit<true>(oe, orr, c - oexcl, v, tile)
-                             : candidate_hit<false>(oe, orr, c - oexcl, v, tile);
+                hit = candidate_hit(oe, orr, c - oexcl, v, tile);
                 gt = v.tile_offset + tile;
             }
             put_keys(a, hit, gt, od, base + (threadIdx.x & ~31) + o);
@@ -511,11 +510,8 @@ __global__ void __launch_bounds__(kBigThreads, kBigBlocksPerSm) tile_sort_big_ke
 void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st)
 {
     constexpr int big_smem = kTileSortSmemKeys * 12;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big_smem);
-        attr = true;
-    }
+    static PerDeviceOnce attr;
+    attr.run([] { cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big_smem); });
     if (a.tiles <= 0) return;
     tile_sort_big_kernel<<<(unsigned)(kBigBlocksPerSm * num_sms), kBigThreads, big_smem, st>>>(a);
 }

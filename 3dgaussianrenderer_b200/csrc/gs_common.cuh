@@ -356,8 +356,8 @@ struct Ell {
     float cx, cy, cs, sn, ex, ey;
 };
 
-// FAST (T_min frames): the divisions by the extents and by the edge length
-// become multiplications by hardware reciprocals; the tests are the same.
+// FAST (the approximate pre-check of ellipse_rect_overlap_clear): the
+// divisions by the extents become multiplications by hardware reciprocals.
 template <bool FAST>
 __device__ __forceinline__ void to_ellipse(const Ell& e, const float px, const float py, float& ox, float& oy,
                                            const float iex, const float iey)
@@ -374,13 +374,12 @@ __device__ __forceinline__ void to_ellipse(const Ell& e, const float px, const f
 
 __device__ __forceinline__ float len2(const float x, const float y) { return x * x + y * y; }
 
-template <bool FAST>
 __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0y, const float v1x, const float v1y)
 {
     const float dx = v1x - v0x, dy = v1y - v0y;
     const float l2 = dx * dx + dy * dy;
     const float num = (-v0x) * dx + (-v0y) * dy;
-    const float t = __saturatef(FAST ? num * rcp_approx(l2) : num / l2);
+    const float t = __saturatef(num / l2);
     const float prx = v0x + t * (v1x - v0x);
     const float pry = v0y + t * (v1y - v0y);
     return len2(prx, pry) < 1.0f;
@@ -394,7 +393,10 @@ __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0
 __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
                                                           const float x1, const float y1);
 
-template <bool FAST = false>
+// ellipseRectOverlap (gaussian_render.cu:250-272): the centre-in-rectangle
+// test, then the other four of the reference's five tests in IEEE
+// arithmetic wherever the approximate evaluation is not clear of the
+// threshold.  Bit-exact with the reference on every input.
 __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x0, const float y0, const float x1,
                                                      const float y1)
 {
@@ -402,53 +404,26 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
     // The reference ORs all five tests, so a centre strictly inside the tile
     // decides the result; skipping the rest changes nothing.
     if (ov) return true;
-    if constexpr (!FAST) {
-        // the approximate evaluation decides whenever it is clear of the
-        // threshold; only near-boundary cases run the IEEE divisions
-        const int clear = ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
-        if (clear >= 0) return clear != 0;
-    }
-    if constexpr (FAST) {
-        // The same five tests on the tile's image in ellipse coordinates, a
-        // parallelogram: corner (x0, y0) maps to a, the x edge to u, the y
-        // edge to v, so the other corners are sums and each edge's squared
-        // length is |u|^2 or |v|^2.
-        const float iex = rcp_approx(e.ex), iey = rcp_approx(e.ey);
-        const float dx0 = x0 - e.cx, dy0 = y0 - e.cy;
-        const float ax = (dx0 * e.cs + dy0 * e.sn) * iex, ay = (dy0 * e.cs - dx0 * e.sn) * iey;
-        const float w = x1 - x0, h = y1 - y0;
-        const float ux = (w * e.cs) * iex, uy = -(w * e.sn) * iey;
-        const float vx = (h * e.sn) * iex, vy = (h * e.cs) * iey;
-        const float rx = ax + 0.5f * (ux + vx), ry = ay + 0.5f * (uy + vy);
-        if (len2(rx, ry) < 1.0f) return true;
-        const float iu = rcp_approx(len2(ux, uy)), iv = rcp_approx(len2(vx, vy));
-        const float bx = ax + ux, by = ay + uy;  // (x1, y0)
-        const float cx = bx + vx, cy = by + vy;  // (x1, y1)
-        const float qx = ax + vx, qy = ay + vy;  // (x0, y1)
-        // segment p + t d, t in [0, 1]: its point nearest the origin inside the unit circle
-        auto edge = [](const float px, const float py, const float dx, const float dy, const float inv) {
-            const float t = __saturatef(-(px * dx + py * dy) * inv);
-            return len2(px + t * dx, py + t * dy) < 1.0f;
-        };
-        return edge(ax, ay, ux, uy, iu) || edge(bx, by, vx, vy, iv) || edge(cx, cy, -ux, -uy, iu) ||
-               edge(qx, qy, -vx, -vy, iv);
-    }
+    // the approximate evaluation decides whenever it is clear of the
+    // threshold; only near-boundary cases run the IEEE divisions
+    const int clear = ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
+    if (clear >= 0) return clear != 0;
     const float iex = 0.0f, iey = 0.0f;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
     const float rcy = y0 + (y1 - y0) * 0.5f;
     float ux, uy;
-    to_ellipse<FAST>(e, rcx, rcy, ux, uy, iex, iey);
+    to_ellipse<false>(e, rcx, rcy, ux, uy, iex, iey);
     ov |= len2(ux, uy) < 1.0f;
     float p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y;
-    to_ellipse<FAST>(e, x0, y0, p0x, p0y, iex, iey);
-    to_ellipse<FAST>(e, x1, y0, p1x, p1y, iex, iey);
-    to_ellipse<FAST>(e, x1, y1, p2x, p2y, iex, iey);
-    to_ellipse<FAST>(e, x0, y1, p3x, p3y, iex, iey);
-    ov |= hits_unit_circle<FAST>(p0x, p0y, p1x, p1y);
-    ov |= hits_unit_circle<FAST>(p1x, p1y, p2x, p2y);
-    ov |= hits_unit_circle<FAST>(p2x, p2y, p3x, p3y);
-    ov |= hits_unit_circle<FAST>(p3x, p3y, p0x, p0y);
+    to_ellipse<false>(e, x0, y0, p0x, p0y, iex, iey);
+    to_ellipse<false>(e, x1, y0, p1x, p1y, iex, iey);
+    to_ellipse<false>(e, x1, y1, p2x, p2y, iex, iey);
+    to_ellipse<false>(e, x0, y1, p3x, p3y, iex, iey);
+    ov |= hits_unit_circle(p0x, p0y, p1x, p1y);
+    ov |= hits_unit_circle(p1x, p1y, p2x, p2y);
+    ov |= hits_unit_circle(p2x, p2y, p3x, p3y);
+    ov |= hits_unit_circle(p3x, p3y, p0x, p0y);
     return ov;
 }
 
@@ -569,7 +544,6 @@ __device__ __forceinline__ void divmod_small(const int c, const int d, int& q, i
 
 // Candidate c of a tile rectangle, row-major (gaussian_render.cu:466-483).
 // Returns true on overlap and the view-local tile index.
-template <bool FAST = false>
 __device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const int c, const ViewParams& v, int& tile)
 {
     int lx, ly;
@@ -579,7 +553,7 @@ __device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const 
     const float ty0 = (float)gy * v.tclip_y - 1.0f;
     const float tx1 = tx0 + v.tclip_x;
     const float ty1 = ty0 + v.tclip_y;
-    if (!ellipse_rect_overlap<FAST>(e, tx0, ty0, tx1, ty1)) return false;
+    if (!ellipse_rect_overlap(e, tx0, ty0, tx1, ty1)) return false;
     // Off-screen candidates only arise from the inverted rectangles of NaN
     // axes; their centre test cannot pass for a visible splat.
     if (gx < 0 || gx >= v.tiles_x || gy < 0 || gy >= v.tiles_y) return false;
@@ -689,7 +663,8 @@ __device__ __forceinline__ int load_flag(const int* p)
 // reported an error, setting *err; the result is then meaningless and the
 // host discards the frame.
 __device__ __forceinline__ uint64_t look_back(const uint64_t* status, const int64_t tile, const int64_t stride,
-                                              const uint32_t epoch, int* err, const int err_code)
+                                              const uint32_t epoch, int* err, const int err_code,
+                                              const int spin_limit = kSpinLimit)
 {
     const uint64_t want = (uint64_t)(epoch & 0xFFFFu) << kEpochShift;
     uint64_t excl = 0;
@@ -698,7 +673,7 @@ __device__ __forceinline__ uint64_t look_back(const uint64_t* status, const int6
     while (j >= 0) {
         const uint64_t s = load_status(status + j * stride);
         if ((s & (kFlagP | kFlagA)) == 0 || (s & kEpochMask) != want) {
-            if (++spins > kSpinLimit || load_flag(err) != 0) {
+            if (++spins > spin_limit || load_flag(err) != 0) {
                 atomicCAS(err, 0, err_code);
                 return excl;
             }

@@ -3,9 +3,63 @@
 
 #include "gs_common.cuh"
 
+#include <atomic>
+
 namespace gs {
 
 constexpr int kErrTimeout = 4;  // GS_ERR_DEVICE_TIMEOUT
+
+// Runs a set-up step once per device.  Function attributes such as
+// cudaFuncAttributeMaxDynamicSharedMemorySize belong to the current
+// device's context, so a kernel that needs more than 48 KB of dynamic
+// shared memory must be opted in on every device it runs on, not once per
+// process.  Devices 0..63 are remembered; higher ones repeat the step on
+// every call (it is idempotent).
+class PerDeviceOnce {
+public:
+    template <class F>
+    void run(F&& f)
+    {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) {
+            cudaGetLastError();
+            dev = -1;
+        }
+        if (dev < 0 || dev >= 64) {
+            f();
+            return;
+        }
+        const uint64_t bit = 1ull << dev;
+        if (done_.load(std::memory_order_acquire) & bit) return;
+        f();
+        done_.fetch_or(bit, std::memory_order_acq_rel);
+    }
+
+private:
+    std::atomic<uint64_t> done_{0};
+};
+
+// Multiprocessor count of the current device (queried once per device).
+inline int device_sm_count()
+{
+    static std::atomic<int> cache[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (dev >= 0 && dev < 64) {
+        const int c = cache[dev].load(std::memory_order_relaxed);
+        if (c > 0) return c;
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) {
+        cudaGetLastError();
+        return 148;
+    }
+    if (dev >= 0 && dev < 64) cache[dev].store(sms, std::memory_order_relaxed);
+    return sms;
+}
 
 // Fused SH + projection + count + scan over (view, Gaussian) pairs.  A block
 // owns one group of 256 Gaussians for `views_per_block` consecutive views;
@@ -52,6 +106,15 @@ struct FrameArgs {
     uint32_t* tile_count;
     unsigned long long* slot_counter;
     int32_t aggregate;  // group same-tile count atomics of a warp (frames with few tiles)
+    // probe outputs (diagnostics and tests; null in ordinary frames): the
+    // projection of every Gaussian of every view at [view * n + caller
+    // index] -- culled Gaussians as centre (-128, -128), depth -128, zero
+    // ellipse and conic -- and the colour of those that reach a tile
+    float2* probe_xy;
+    float* probe_z;
+    float4* probe_ell;
+    float4* probe_conic;
+    float4* probe_color;
 };
 
 // Bucket emission: every overlap of slot s is written as
@@ -72,7 +135,6 @@ struct BucketEmitArgs {
     uint64_t* keys;
     int64_t capacity;
     int32_t aggregate;               // group same-tile cursor atomics of a warp (frames with few tiles)
-    int32_t fast;                    // re-test candidates as the frame kernel did (T_min frames: FAST)
 };
 
 // Frames of at most this many tiles (all views) group the same-tile atomics
@@ -137,7 +199,6 @@ struct EmitArgs {
     uint64_t* keys;
     int32_t* values;
     int64_t capacity;
-    int32_t fast;  // re-test candidates as the frame kernel did (T_min frames: FAST)
 };
 
 // Raster record of one (view, Gaussian) for GS_TERM_TMIN, written by the

@@ -19,8 +19,11 @@
 //    the previous call's contents: each call clears the words that must
 //    start at zero.  Calls whose work overlaps on the GPU race and corrupt
 //    each other's results: serialise them (one stream, or one call at a time);
-//  * the first call on a device looks up the array's device address with
-//    cudaGetSymbolAddress; make that first call before any stream capture.
+//  * every call looks up the array's device address with
+//    cudaGetSymbolAddress; the first call on a device also loads the module,
+//    so make that first call before any stream capture.  After a
+//    cudaDeviceReset the module comes back with a fresh array at a possibly
+//    new address, which the next call picks up.
 #include "gs_kernels.h"
 #include "../../include/gs_b200.h"
 
@@ -93,17 +96,21 @@ GS_API int gs_stage_sort_noalloc(int64_t num_keys, int32_t key_bits, uint64_t* d
     {
         std::lock_guard<std::mutex> lock(g_mu);
         DeviceState& d = g_dev[dev];
-        if (!d.ptr) {
-            // once per device, with that device current: the host-side name of
-            // the array is not a device address
-            void* p = nullptr;
-            const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                g_err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
-                return GS_ERR_CUDA;
-            }
+        // with this device current: the host-side name of the array is not a
+        // device address.  The first call on a device loads the module; later
+        // calls only read the address back, and a changed address (the
+        // context was reset, which reloads the module with a zeroed array)
+        // restarts the epochs.
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            g_err = std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e);
+            return GS_ERR_CUDA;
+        }
+        if (d.ptr != static_cast<NoAllocScratch*>(p)) {
             d.ptr = static_cast<NoAllocScratch*>(p);
+            d.epoch = 1;
         }
         s = d.ptr;
         if (d.epoch + (uint32_t)passes > 0xFFFFu) {
@@ -130,7 +137,7 @@ GS_API int gs_stage_sort_noalloc(int64_t num_keys, int32_t key_bits, uint64_t* d
     ss.err = &s->err;
     ss.max_tiles = kNoAllocMaxTiles;
     const int done = gs::launch_sort(d_keys, d_values, d_keys_alt, d_values_alt, num_keys, nullptr, key_bits, ss, epoch,
-                                     148, st);
+                                     gs::device_sm_count(), st);
     cudaError_t e = cudaGetLastError();
     int err = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&err, &s->err, sizeof(int), cudaMemcpyDeviceToHost, st);

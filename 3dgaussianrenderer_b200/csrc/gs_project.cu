@@ -99,7 +99,6 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
 // and when a frame has few tiles, many atomics on one address serialise.
 // With many tiles the atomics spread out and the grouping costs more than
 // it saves.
-template <bool FAST = false>
 __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
                                                uint32_t& mask, uint32_t* tile_count = nullptr,
                                                const bool aggregate = false)
@@ -126,7 +125,7 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
         const int oexcl = __shfl_sync(kFull, w.excl, o);
         bool hit = false;
         int tile = 0;
-        if (c < w.total) hit = candidate_hit<FAST>(oe, orr, c - oexcl, v, tile);
+        if (c < w.total) hit = candidate_hit(oe, orr, c - oexcl, v, tile);
         const unsigned bal = __ballot_sync(kFull, hit);
 if (tile_count && hit) {
             if (aggregate) {
@@ -267,11 +266,13 @@ __global__ void __launch_bounds__(256, (DEG >= 3 && !FAST) ? 3 : 4) frame_projec
         int cand = 0;
         Splat s;
         float4 col = cin;
+        bool projected = false;
         if (valid) {
             // outside the frustum: culled, no tile (whole warps of a
             // spatially ordered scene skip the projection together)
             const ViewPos w = view_position<FAST>(p, v);
             if (in_frustum(w)) {
+                projected = true;
                 s = project_gaussian<FAST>(w, sr, v);
                 e = {s.x, s.y, s.cs, s.sn, s.ex, s.ey};
                 r = tile_rect(e, v);
@@ -279,7 +280,9 @@ __global__ void __launch_bounds__(256, (DEG >= 3 && !FAST) ? 3 : 4) frame_projec
             }
         }
         uint32_t mask;
-        const int hits = warp_count_hits<FAST>(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr, a.aggregate != 0);
+        // the overlap test is the reference's in every mode: the tile lists
+        // of the projected floats are exactly those of the reference's build
+        const int hits = warp_count_hits(e, r, cand, v, mask, BUCKET ? a.tile_count : nullptr, a.aggregate != 0);
         int64_t o_out = o;  // where this item's outputs go
         if (BUCKET) {
             const unsigned bal = __ballot_sync(kFull, hits > 0);
@@ -296,6 +299,20 @@ __global__ void __launch_bounds__(256, (DEG >= 3 && !FAST) ? 3 : 4) frame_projec
         }
         if (valid) {
             const int64_t o = o_out;
+            if (a.probe_xy) {
+                const int64_t q = (int64_t)view * a.n + gid;
+                if (projected) {
+                    a.probe_xy[q] = make_float2(s.x, s.y);
+                    a.probe_z[q] = s.z;
+                    a.probe_ell[q] = make_float4(s.cs, s.sn, s.ex, s.ey);
+                    a.probe_conic[q] = make_float4(s.ca, s.cb, s.cc, 0.0f);
+                } else {
+                    a.probe_xy[q] = make_float2(-128.0f, -128.0f);
+                    a.probe_z[q] = -128.0f;
+                    a.probe_ell[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                    a.probe_conic[q] = make_float4(0.f, 0.f, 0.f, 0.f);
+                }
+            }
             if (hits > 0) {
                 // the colour only matters for items that reach a tile, so the
                 // SH evaluation runs after the overlap test
@@ -304,6 +321,7 @@ __global__ void __launch_bounds__(256, (DEG >= 3 && !FAST) ? 3 : 4) frame_projec
                     const float3 c = sh_color<DEG, false>(d.x, d.y, d.z, s_sh + threadIdx.x, 256);
                     col = make_float4(c.x, c.y, c.z, p.w);
                 }
+                if (a.probe_color) a.probe_color[(int64_t)view * a.n + gid] = col;
                 a.z[o] = s.z;
                 a.rect[o] = pack_rect(r);
                 a.hitmask[o] = mask;
@@ -469,8 +487,7 @@ __global__ void __launch_bounds__(256) emit_kernel(EmitArgs a)
         bool hit = false;
         int tile = 0;
         if (c < w.total)
-            hit = a.fast ? candidate_hit<true>(oe, orr, c - oexcl, a.views[oview], tile)
-                         : candidate_hit<false>(oe, orr, c - oexcl, a.views[oview], tile);
+            hit = candidate_hit(oe, orr, c - oexcl, a.views[oview], tile);
         const unsigned bal = __ballot_sync(kFull, hit);
         if (hit) {
             const unsigned omask = lane_range_mask(max(oexcl - base, 0), min(oincl - base, 32));
@@ -514,12 +531,11 @@ static void launch_frame_deg(const FrameArgs& a, cudaStream_t st)
 {
     constexpr int NCOEF = DEG >= 0 ? 3 * (DEG + 1) * (DEG + 1) : 0;
     constexpr int smem = NCOEF * 256 * (int)sizeof(float);
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    attr.run([] {
         cudaFuncSetAttribute(frame_project_kernel<DEG, BUCKET, FAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              smem);
-        attr = true;
-    }
+    });
     frame_project_kernel<DEG, BUCKET, FAST><<<(unsigned)a.num_tiles, 256, smem, st>>>(a);
 }
 

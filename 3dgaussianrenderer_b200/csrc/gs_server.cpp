@@ -80,6 +80,7 @@ struct gs_server {
     std::vector<std::unique_ptr<Worker>> workers;
     std::thread scheduler;
     bool stop = false;
+    bool paused = false;  // gs_server_pause: requests queue, none is dispatched
     int64_t resident_bytes = 0;
     // statistics
     std::vector<double> latencies;
@@ -199,12 +200,13 @@ void scheduler_loop(gs_server* S)
     for (;;) {
         S->cv_sched.wait(lk, [&] {
             if (S->stop) return true;
-            if (S->pending.empty()) return false;
+            if (S->pending.empty() || S->paused) return false;
             for (auto& w : S->workers)
                 if (!w->has_batch) return true;
             return false;
         });
         if (S->stop) return;
+        if (S->paused) continue;
         Worker* free_w = nullptr;
         for (auto& w : S->workers)
             if (!w->has_batch) {
@@ -389,6 +391,34 @@ GS_API int gs_server_wait(gs_server* S, int64_t id, double timeout_ms, double* o
     S->done.erase(id);
     if (out_latency_ms) *out_latency_ms = d.latency_ms;
     return d.status;
+}
+
+GS_API int gs_server_cancel(gs_server* S, int64_t id)
+{
+    if (!S) return GS_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        auto it = std::find_if(S->pending.begin(), S->pending.end(), [&](const Request& r) { return r.id == id; });
+        // already handed to a worker (its batch is on the device), finished,
+        // or unknown: nothing to cancel
+        if (it == S->pending.end()) return GS_ERR_INVALID;
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - it->submitted).count();
+        S->done[id] = Done{GS_ERR_CANCELLED, ms};
+        S->pending.erase(it);
+    }
+    S->cv_done.notify_all();
+    return GS_OK;
+}
+
+GS_API int gs_server_pause(gs_server* S, int32_t paused)
+{
+    if (!S) return GS_ERR_INVALID;
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->paused = paused != 0;
+    }
+    S->cv_sched.notify_all();
+    return GS_OK;
 }
 
 GS_API int gs_server_get_stats(gs_server* S, gs_server_stats* out)

@@ -229,11 +229,10 @@ static void launch_pass_t(const SortPassArgs& a, int64_t num_items, cudaStream_t
 {
     constexpr int tile = THREADS * IPT;
     constexpr int smem = tile * 12;
-    static bool attr = false;
-    if (!attr) {
+    static PerDeviceOnce attr;
+    attr.run([] {
         cudaFuncSetAttribute(onesweep_kernel<THREADS, IPT, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-        attr = true;
-    }
+    });
     const int64_t tiles = (num_items + tile - 1) / tile;
     onesweep_kernel<THREADS, IPT, MINB><<<(unsigned)tiles, THREADS, smem, st>>>(a);
 }
@@ -264,12 +263,11 @@ int launch_sort(const uint64_t* keys_in, const int32_t* vals_in, uint64_t* keys_
 {
     const int passes = sort_passes(key_bits);
     if (num_items <= 0 || passes == 0) return 0;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static PerDeviceOnce attr;
+    attr.run([] {
         cudaFuncSetAttribute(sort_hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              8 * kMaxPasses * kRadix * 4);
-        attr_set = true;
-    }
+    });
     cudaMemsetAsync(s.hist, 0, sizeof(uint32_t) * kMaxPasses * kRadix, st);
     cudaMemsetAsync(s.counters, 0, sizeof(unsigned long long) * kMaxPasses, st);
     const int hist_blocks = (int)std::min<int64_t>((int64_t)num_sms * 4, std::max<int64_t>(1, (num_items + 4095) / 4096));
@@ -316,7 +314,7 @@ void launch_ranges(const uint64_t* keys, int64_t num_items, const int64_t* d_num
                    cudaStream_t st)
 {
     if (num_items <= 0) return;
-    const int64_t blocks = std::min<int64_t>((num_items + 255) / 256, 148 * 32);
+    const int64_t blocks = std::min<int64_t>((num_items + 255) / 256, (int64_t)device_sm_count() * 32);
     ranges_kernel<<<(unsigned)blocks, 256, 0, st>>>(keys, num_items, d_num_items, ranges);
 }
 

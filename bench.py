@@ -59,6 +59,29 @@ def make_workload(gs, rank=0):
     return sc, cams
 
 
+def scenes_module():
+    """The seeded scene generator (plain numpy), loaded from its file so that
+    the reference arm never loads the product library."""
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("gs_scenes", os.path.join(ROOT, "3dgaussianrenderer_b200",
+                                                                            "scenes.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def make_workload_reference(O, rank=0):
+    """make_workload's scene and cameras built without the product library:
+    the same generator, cameras from the oracle's look-at (bit-identical to
+    gs_camera_look_at, tests/test_oracle_cpu.py)."""
+    sc_mod = scenes_module()
+    sc = sc_mod.config_scene("batch3m")
+    eyes = sc_mod.orbit_ring(VIEWS, RING_RADIUS, seed=1000 + rank)
+    cams = [O.look_at(e, (0, 0, 0), (0, 1, 0), 50.0, *sc_mod.BATCH_RESOLUTIONS[i % 3], 0.1, 100.0)
+            for i, e in enumerate(eyes)]
+    return sc_mod, sc, cams
+
+
 class Clocks:
     """nvidia-smi sampling (100 ms period) kept to the samples taken inside
     the timed region [mark_start(), mark_end()]."""
@@ -145,12 +168,13 @@ SERVE_SCENES = [200_000, 500_000, 1_000_000, 1_000_000, 2_000_000, 2_000_000, 3_
 SERVE_RES = [(1280, 720), (1920, 1080), (2560, 1440)]
 
 
-def run_serving(gs, rank, rate=500.0, requests=10_000, budget_gb=150, max_batch=16, workers=2):
-    """Serving workload: 8 resident scenes, Poisson request stream at `rate`
-    req/s (scene uniform, pose uniform on a radius-12 sphere, resolution
-    uniform over 720p/1080p/1440p), admitted against a device-memory budget;
-    `requests` requests (about 20 s at 500 req/s).  Latency = submit ->
-    image in host memory."""
+def run_serving(gs, rank, rates=(500.0, 2000.0, 5000.0), requests=10_000, budget_gb=150, max_batch=16, workers=2):
+    """Serving workload: 8 resident scenes, Poisson request streams at each
+    of `rates` req/s in turn (scene uniform, pose uniform on a radius-12
+    sphere, resolution uniform over 720p/1080p/1440p), admitted against a
+    device-memory budget; `requests` requests per rate (about 20 s at 500
+    req/s, the configuration's rate; the faster streams show continuous
+    batching under load).  Latency = submit -> image in host memory."""
     srv = gs.Server(0, budget_bytes=budget_gb << 30, max_batch_views=max_batch, num_workers=workers)
     ids = []
     for k, n in enumerate(SERVE_SCENES):
@@ -183,31 +207,38 @@ def run_serving(gs, rank, rate=500.0, requests=10_000, budget_gb=150, max_batch=
             burst.append(srv.submit(ids[-1], cam, bufs[k]))
         for r in burst:
             srv.wait(r)
-    srv.reset_stats()
-    t0 = time.perf_counter()
-    t_next = t0
-    slot = 0
-    count = 0
-    while count < requests:
-        t_next += rng.exponential(1.0 / rate)
-        s, cam = make_request()
-        if inflight[slot] is not None:
-            srv.wait(inflight[slot])
-        delay = t_next - time.perf_counter()
-        if delay > 0:
-            time.sleep(delay)
-        inflight[slot] = srv.submit(s, cam, bufs[slot])
-        slot = (slot + 1) % ring
-        count += 1
-    for r in inflight:
-        if r is not None:
-            srv.wait(r)
-    st = srv.stats()
+    legs = []
+    for rate in rates:
+        srv.reset_stats()
+        t0 = time.perf_counter()
+        t_next = t0
+        slot = 0
+        count = 0
+        while count < requests:
+            t_next += rng.exponential(1.0 / rate)
+            s, cam = make_request()
+            if inflight[slot] is not None:
+                srv.wait(inflight[slot])
+                inflight[slot] = None
+            delay = t_next - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            inflight[slot] = srv.submit(s, cam, bufs[slot])
+            slot = (slot + 1) % ring
+            count += 1
+        for k, r in enumerate(inflight):
+            if r is not None:
+                srv.wait(r)
+                inflight[k] = None
+        st = srv.stats()
+        legs.append({"views_per_s": st["views_per_s"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                     "mean_ms": st["mean_ms"], "requests": count, "rate_req_s": rate, "max_batch": st["max_batch"],
+                     "batches": st["batches_done"]})
     srv.close()
-    return {"views_per_s": st["views_per_s"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "mean_ms": st["mean_ms"], "requests": count, "rate_req_s": rate, "max_batch": st["max_batch"],
-            "batches": st["batches_done"], "budget_gb": budget_gb, "workers": workers,
-            "scenes_m": [n / 1e6 for n in SERVE_SCENES]}
+    out = dict(legs[0], budget_gb=budget_gb, workers=workers, in_flight_limit=ring,
+               scenes_m=[n / 1e6 for n in SERVE_SCENES])
+    out["sweep"] = legs[1:]
+    return out
 
 
 def job_views_per_s(local_ms: float, views_per_rank: int, steps: int, world: int, device=None) -> tuple:
@@ -253,16 +284,38 @@ def run_ref1024(gs, ctx, sc, dev, stream, frames=30):
             "reference-compatible mode, single view"}
 
 
+def run_ref_cuda_1024(sc, frames=30):
+    """The reference's own CUDA frame (its kernels built from
+    core/gaussian_render.cu into oracle/_ref/libgsref.so, run by the headless
+    frame loop of app/main.cpp:360-432) on the same 3M-Gaussian scene and
+    1024x1024 camera as run_ref1024, on the same GPU, in the same process:
+    the comparison the plain path's >= 1.5x target is quoted against.  Median
+    of `frames` frames, CUDA events around each whole frame.  None when the
+    harness was not built (the reference sources were absent)."""
+    import oracle
+    if not os.path.exists(oracle.REF_LIB):
+        return None
+    O = oracle.get()
+    sc_mod = scenes_module()
+    eye = sc_mod.orbit_ring(64, RING_RADIUS, seed=1000)[0]
+    cam = O.look_at(eye, (0, 0, 0), (0, 1, 0), 50.0, 1024, 1024, 0.1, 100.0)
+    ref = oracle.Ref()
+    _, k, times, stage = ref.time_frames(sc["pos4"], sc["sr4"], sc_mod.grouped_sh(sc["sh"]), 3, cam, frames)
+    return {"frame_ms": float(np.median(times)), "keys": k,
+            "stage_ms_sh_clip_build_sort_ranges_raster": stage,
+            "workload": "the reference's CUDA frame loop (SH degree <= 2, tile-wide T <= 0.02), same scene and "
+                        "camera"}
+
+
 def run_reference(args, rank, world):
-    import torch.distributed as dist
     if rank != 0:
         return
-    gs = importlib.import_module("3dgaussianrenderer_b200")
-    sc, cams = make_workload(gs)
     import oracle
     O = oracle.get()
-    sh = gs.scenes.grouped_sh(sc["sh"])
-    rc = gs.RenderConfig()
+    sc_mod, sc, cams = make_workload_reference(O)
+    sh = sc_mod.grouped_sh(sc["sh"])
+    # the frame options of the GPU leg: SH degree 3, per-pixel T < 1e-4, 16x16 tiles
+    rc = oracle.gso_cfg(3, 1, 1e-4, 16, 16)
     for w in range(args.warmup):
         O.render(sc, sh, cams[w % VIEWS], rc)
     times = []
@@ -397,7 +450,21 @@ def run_ours(args, rank, world, local_rank):
 
     ref1024 = None
     if not args.no_plain:
+        clk1024 = Clocks(local_rank) if rank == 0 else None
+        if clk1024:
+            clk1024.mark_start()
         ref1024 = run_ref1024(gs, ctx, sc, dev, stream)
+        if rank == 0 and not args.no_ref_cuda:
+            # the reference's own CUDA frame on the same scene, camera and GPU
+            rc_ref = run_ref_cuda_1024(sc)
+            if rc_ref:
+                ref1024["ref_cuda_1024_frame_ms"] = rc_ref["frame_ms"]
+                ref1024["ref_cuda_1024"] = rc_ref
+                ref1024["speedup_vs_ref_cuda"] = rc_ref["frame_ms"] / ref1024["frame_ms"]
+                ref1024["same_keys_as_ref_cuda"] = rc_ref["keys"] == ref1024["keys"]
+        if clk1024:
+            clk1024.mark_end()
+            ref1024["clocks"] = clk1024.stop()
 
     served = None
     if not args.no_serve:
@@ -433,28 +500,30 @@ def run_ours(args, rank, world, local_rank):
     dom = max(per, key=per.get)
     cpu = cpu_baseline(gs, sc, cams, rc, sample_views=1) if (world == 1 and not args.no_cpu) else None
     # The dominant kernel, the T_min raster, against the FP32 pipe (it is
-    # neither HBM- nor tensor-bound), for view 0 rendered alone: work = 11
-    # FP32 lane operations per (pixel, entry) evaluation of the packed blend
-    # (exponent: 2 fma + the column terms; w; 3 colour fma; T update), the
+    # neither HBM- nor tensor-bound), for view 0 rendered alone, with the
+    # scope table's fixed count: 20 FP32 flop per (pixel, splat) blend
+    # evaluation (the reference's expression: offset, quadratic form,
+    # exponent scale, alpha, three colour multiply-adds and the
+    # transmittance update, a multiply-add counted as 2), over the
     # evaluations the GPU's warp-culled walk executes as counted by the
     # oracle's model of it; time = the raster stage; peak = 148 SMs x 128
-    # FP32 lanes x the SM clock sampled during the timed region (nominal:
-    # there is no measured FP32 peak).  The oracle's count without the cull
-    # (every entry until T < t_min) is given beside it.  traffic: DRAM bytes
-    # of an ncu capture of the same single-view launch.
+    # FP32 lanes x 2 flop x the SM clock sampled during the timed region
+    # (nominal: there is no measured FP32 peak).  The oracle's count without
+    # the cull (every entry until T < t_min) is given beside it.  traffic:
+    # DRAM bytes of an ncu capture of the same single-view launch.
     raster_roof = None
     if cpu and cpu.get("block_evals_view0") and raster_view0_ms:
         clk_mhz = (clocks or {}).get("sm_mhz") or 1965.0
-        peak_gops = 148 * 128 * clk_mhz * 1e6 / 1e9
-        ach = 11.0 * cpu["block_evals_view0"] / (raster_view0_ms / 1e3) / 1e9
+        peak_gflops = 148 * 128 * 2 * clk_mhz * 1e6 / 1e9
+        ach = 20.0 * cpu["block_evals_view0"] / (raster_view0_ms / 1e3) / 1e9
         raster_roof = {"bound": "fp32", "kernel": "raster_rec (T_min records, per-tile sort fused)",
-                       "achieved": ach, "peak": peak_gops, "unit": "Gop/s", "frac": ach / peak_gops,
+                       "achieved": ach, "peak": peak_gflops, "unit": "GFLOP/s", "frac": ach / peak_gflops,
                        # captured with 16x16 tiles
                        "traffic": RASTER_VIEW0_TRAFFIC if (rc.tile_w, rc.tile_h) == (16, 16) else None,
                        "evals_executed": cpu["block_evals_view0"], "evals_unculled": cpu["evals_view0"],
-                       "ops_per_eval": 11, "raster_ms": raster_view0_ms,
+                       "flop_per_eval": 20, "raster_ms": raster_view0_ms,
                        "view": f"view 0 ({cams[0].GetWidth()}x{cams[0].GetHeight()}) rendered alone",
-                       "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x sampled SM clock"}
+                       "peak_kind": "nominal: 148 SMs x 128 FP32 lanes x 2 flop x sampled SM clock"}
     roof = raster_roof or frame_roof
     roof = dict(roof, stage_ms=per, dominant_stage=dom)
     line = {
@@ -494,6 +563,8 @@ def main():
     ap.add_argument("--no-plain", action="store_true", help="skip the single-view leg (profiling runs)")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg (profiling runs)")
     ap.add_argument("--no-autotune", action="store_true", help="default knobs (16x16 tiles, 16 views per block)")
+    ap.add_argument("--no-ref-cuda", action="store_true",
+                    help="skip the reference's own CUDA frame beside the 1024x1024 plain frame")
     ap.add_argument("--only-ref1024", action="store_true",
                     help="time only the reference-compatible 1024x1024 single-view frame (profiling case)")
     ap.add_argument("--views", type=int, default=VIEWS,

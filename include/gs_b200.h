@@ -47,7 +47,8 @@ enum {
     GS_ERR_CAPACITY = 3,       /* a caller-sized buffer is too small */
     GS_ERR_DEVICE_TIMEOUT = 4, /* a bounded device wait gave up */
     GS_ERR_CUDA = 5,           /* other CUDA error (see gs_last_error_string) */
-    GS_ERR_NO_DEVICE = 6       /* no usable sm_100 device */
+    GS_ERR_NO_DEVICE = 6,      /* no usable sm_100 device */
+    GS_ERR_CANCELLED = 7       /* a server request cancelled before it was rendered */
 };
 
 enum { GS_TERM_REFERENCE = 0, GS_TERM_TMIN = 1 };
@@ -259,8 +260,10 @@ GS_API int gs_stage_project(int64_t n, const float* d_position, const float* d_s
 
 /* buildTileList (gaussian_render.cu:312-589).  Exact: counts every
  * Gaussian's overlapping tiles, scans, and emits keys in Gaussian order.
- * Synchronises once to read K into *out_num_keys.  Returns
- * GS_ERR_CAPACITY (and writes nothing) when K > capacity. */
+ * Synchronises once to read K into *out_num_keys.  When K > capacity it
+ * writes the first `capacity` keys (in Gaussian order; the reference
+ * truncates in atomic order) and returns GS_ERR_CAPACITY with the exact K,
+ * so the caller can grow the lists. */
 GS_API int gs_stage_build(gs_ctx* ctx, int64_t n, const float* d_xy, const float* d_z, const float* d_ellipse,
                    const gs_camera* cam, const gs_render_cfg* cfg, uint64_t* d_keys, int32_t* d_values,
                    int64_t capacity, int64_t* out_num_keys, void* stream);
@@ -280,8 +283,10 @@ GS_API int gs_stage_sort(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, uint64
  * the call allocates nothing.  At most gs_stage_sort_noalloc_max_keys()
  * (4,194,304) keys; more returns GS_ERR_CAPACITY.  All calls share the array:
  * calls that overlap on the GPU race, so serialise them.  The first call on
- * a device resolves the array's address; make it before any stream capture.
- * Synchronises `stream` before returning. */
+ * a device loads the array's module and resolves its address; make it
+ * before any stream capture.  Every call re-reads the address, so the call
+ * keeps working after a cudaDeviceReset.  Synchronises `stream` before
+ * returning. */
 GS_API int gs_stage_sort_noalloc(int64_t num_keys, int32_t key_bits, uint64_t* d_keys, int32_t* d_values,
                                  uint64_t* d_keys_alt, int32_t* d_values_alt, int32_t* out_selector, void* stream);
 GS_API int64_t gs_stage_sort_noalloc_max_keys(void);
@@ -328,8 +333,17 @@ GS_API int gs_server_add_scene(gs_server* server, int64_t n, const float* h_posi
 /* Non-blocking; h_rgba (4*W*H bytes, host) is written before the request completes. */
 GS_API int gs_server_submit(gs_server* server, int32_t scene_id, const gs_camera* cam, uint8_t* h_rgba,
                             int64_t* out_request_id);
-/* Waits up to timeout_ms; returns the request's status (GS_ERR_DEVICE_TIMEOUT if not done). */
+/* Waits up to timeout_ms; returns the request's status (GS_ERR_DEVICE_TIMEOUT if not done,
+ * GS_ERR_CANCELLED if it was cancelled). */
 GS_API int gs_server_wait(gs_server* server, int64_t request_id, double timeout_ms, double* out_latency_ms);
+/* Cancels a request that is still queued: it completes at once with status
+ * GS_ERR_CANCELLED and its host buffer is never written.  GS_ERR_INVALID when
+ * the request is unknown, finished, or already part of a batch on the device
+ * (which is never interrupted). */
+GS_API int gs_server_cancel(gs_server* server, int64_t request_id);
+/* paused = 1: submitted requests queue and no new batch is dispatched
+ * (batches already on the device finish); 0: dispatching resumes. */
+GS_API int gs_server_pause(gs_server* server, int32_t paused);
 GS_API int gs_server_get_stats(gs_server* server, gs_server_stats* out);
 GS_API int gs_server_reset_stats(gs_server* server);
 
@@ -350,6 +364,60 @@ GS_API int gs_ply_read(const char* path, float* h_position, float* h_scale_rotat
  * reads back; SH scenes get f_rest_* (channel-major). */
 GS_API int gs_ply_write(const char* path, int64_t n, const float* h_position, const float* h_scale_rotation,
                         const float* h_color, const float* h_sh_grouped, int32_t sh_degree);
+
+/* ---- frame probe (diagnostics and tests) ------------------------------- */
+/* No counterpart in the reference, whose stages leave every intermediate
+ * buffer with the caller; the fused frame keeps them internal, and the probe
+ * exposes what the parity tests compare with the reference's stages.
+ * Device outputs per (view, Gaussian), num_views * n entries each, at
+ * view * n + the caller's index of the Gaussian: */
+typedef struct gs_frame_probe {
+    float* d_xy;      /* float2 clip-space centre; frustum-culled: (-128, -128) */
+    float* d_z;       /* clip-space depth; culled: -128 */
+    float* d_ellipse; /* float4 (cos, sin, extent.x, extent.y) as the tile lists use it; culled: 0 */
+    float* d_conic;   /* float4 (a, b, c, 0); culled: 0 */
+    float* d_color;   /* float4 (r, g, b, opacity) of the Gaussians that reach a tile (others untouched); may be NULL */
+} gs_frame_probe;
+
+/* Renders like gs_render_batch with GS_ORDER_BUCKETS (never from a captured
+ * graph) and writes the probe outputs.  The projection and tile lists are
+ * those of an ordinary frame with the same options. */
+GS_API int gs_probe_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
+                          const gs_render_cfg* cfg, uint8_t* const* d_rgba, const gs_frame_probe* probe,
+                          gs_stats* stats, void* stream);
+/* Copies the tile lists of the context's last GS_ORDER_BUCKETS frame to host
+ * memory (GS_ERR_INVALID when a stage call or a onesweep frame has reused
+ * the buffers since).  out_sizes = (tiles T, keys K, slots S);
+ * *out_fused_cap = the largest tile the raster CTA sorts itself.
+ *   h_ranges[2T]    first and one-past-last key of every tile (all views'
+ *                   tiles, view after view);
+ *   h_keys[K]       the tiles' keys as emitted, (depth bits << 32 | slot),
+ *                   in any order inside a tile: the raster CTA of a tile of
+ *                   at most fused_cap keys orders them by (depth, index);
+ *   h_order[K]      for the larger tiles, the slots in blend order (sorted
+ *                   ahead of the raster); meaningless for the others;
+ *   h_slot_index[S] view * n + caller index of each slot.
+ * Any output may be NULL.  Synchronous. */
+GS_API int gs_probe_tile_lists(gs_ctx* ctx, int32_t* h_ranges, int64_t ranges_capacity, uint64_t* h_keys,
+                               int32_t* h_order, int64_t keys_capacity, int32_t* h_slot_index, int64_t slots_capacity,
+                               int64_t out_sizes[3], int32_t* out_fused_cap);
+
+/* ---- failure-path test hooks -------------------------------------------- */
+/* No counterpart in the reference, which exits the process on any CUDA
+ * error (core/cuda_error_check.h:2-11).  These let tests exercise the error
+ * paths that replace it without faulting a GPU. */
+/* After `skip` more device buffer allocations of contexts and scenes
+ * succeed, the next `count` fail as if the device were out of memory
+ * (process-wide; count = 0 clears the hook).  The failing call returns
+ * GS_ERR_OOM and the context stays usable. */
+GS_API void gs_test_fail_allocations(int32_t skip, int32_t count);
+/* Injected failures not yet consumed. */
+GS_API int32_t gs_test_pending_allocation_failures(void);
+/* Runs one bounded device wait on a word nobody publishes (the decoupled
+ * look-back every scan and sort pass uses) with a limit of `spin_limit`
+ * polls (1 .. 4194304).  Returns GS_ERR_DEVICE_TIMEOUT when the wait gave up
+ * and reported it, as it must; the context stays usable. */
+GS_API int gs_test_bounded_wait(int32_t spin_limit, void* stream);
 
 /* Number of tiles of a W x H image with the cfg's tile shape. */
 GS_API int64_t gs_num_tiles(int32_t width, int32_t height, const gs_render_cfg* cfg);

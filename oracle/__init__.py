@@ -19,6 +19,9 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_LIB = os.path.join(HERE, "_build", "libgsoracle.so")
 REF_LIB = os.path.join(HERE, "_ref", "libgsref.so")
+# the same frame-loop harness over include/gs_stage_compat.hpp (gs_b200
+# behind the reference's stage declarations): the stage-API drop-in
+COMPAT_LIB = os.path.join(HERE, "_ref", "libgscompat.so")
 
 _P = ctypes.c_void_p
 _I32 = ctypes.c_int32
@@ -49,11 +52,15 @@ class gso_cfg(ctypes.Structure):
 
 def camera(cam) -> gso_camera:
     """Oracle camera from a product Camera / gs_camera (identical layout)."""
+    if isinstance(cam, gso_camera):
+        return cam
     c = getattr(cam, "c", cam)
     return gso_camera.from_buffer_copy(bytes(c))
 
 
 def cfg(rc) -> gso_cfg:
+    if isinstance(rc, gso_cfg):
+        return rc
     return gso_cfg(rc.sh_max_degree, rc.termination, rc.t_min, rc.tile_w, rc.tile_h)
 
 
@@ -89,6 +96,7 @@ class Oracle:
             "gso_raster": (None, [pc, pg, _P, _P, _P, _P, _P, _P, _P]),
             "gso_render": (_I64, [_I64, _P, _P, _P, _P, _I32, _I32, pc, pg, _P, _I64, _P, _P]),
             "gso_set_count_block_evals": (None, [_I32]),
+            "gso_look_at": (None, [pc, _P, _P, _P, ctypes.c_float, _I32, _I32, ctypes.c_float, ctypes.c_float]),
             "gso_block_evals": (_I64, []),
         }
         for name, (res, args) in sig.items():
@@ -107,6 +115,17 @@ class Oracle:
 
     def set_threads(self, n: int):
         self.lib.gso_set_threads(n)
+
+    def look_at(self, eye, target, up=(0.0, 1.0, 0.0), fovy_deg=50.0, width=1024, height=1024, near=0.1,
+                far=100.0) -> gso_camera:
+        """A camera built by the oracle alone (no product library), with the
+        same float arithmetic as gs_camera_look_at: fovy in degrees, converted
+        to radians in double precision and rounded to float."""
+        cam = gso_camera()
+        e, t, u = (np.ascontiguousarray(x, np.float32) for x in (eye, target, up))
+        self.lib.gso_look_at(ctypes.byref(cam), _addr(e), _addr(t), _addr(u), float(np.radians(fovy_deg)),
+                             int(width), int(height), float(near), float(far))
+        return cam
 
     def count_block_evals(self, on: bool):
         """Counts, in later T_min rasters, the (pixel, entry) evaluations the
@@ -261,9 +280,60 @@ class Ref:
             "gsref_probe_key": (ctypes.c_int, [ctypes.c_int, _P, _P, _P]),
         }
         for name, (res, args) in sig.items():
+            if name.startswith("gsref_probe_") and not hasattr(L, name):
+                continue  # the stage-compat build has no device-helper probes
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args
+
+    def time_frames(self, pos4, sr4, sh_grouped, sh_degree, cam, frames=30, warmup=3):
+        """Renders the scene `warmup + frames` times with the reference's own
+        frame loop (gsref_render_frame: every stage behind its blocking
+        CudaTimer, the tile counter read back after the build, as
+        app/main.cpp:360-432 runs it), growing the tile lists like the
+        reference whenever they saturate.  Returns (image, K, per-frame ms of
+        the timed frames (CUDA events around each whole frame), mean stage ms
+        (sh, clip, build, sort, ranges, raster))."""
+        import torch
+        n = int(pos4.shape[0])
+        dev = "cuda"
+        t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        pos, sr = t(pos4), t(sr4)
+        sh = t(sh_grouped)
+        color = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        xy = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+        z = torch.zeros(n, dtype=torch.float32, device=dev)
+        conic = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        ell = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+        img = torch.zeros((self.SCREEN, self.SCREEN, 4), dtype=torch.uint8, device=dev)
+        ranges = torch.zeros(2 * self.TILES, dtype=torch.int32, device=dev)
+        cap = 8 * n  # app/main.cpp:305
+        cam56 = self.camera56(cam)
+        sh_count = 3 * (sh_degree + 1) ** 2
+        while True:
+            keys = [torch.zeros(cap, dtype=torch.int64, device=dev) for _ in range(2)]
+            vals = [torch.zeros(cap, dtype=torch.int32, device=dev) for _ in range(2)]
+            times, stage = [], []
+            k = 0
+            for f in range(frames + warmup):
+                ms = (ctypes.c_float * 6)()
+                fms = ctypes.c_float(0)
+                sel = ctypes.c_int(0)
+                k = self.lib.gsref_render_frame(cam56.ctypes.data, pos.data_ptr(), sr.data_ptr(), color.data_ptr(),
+                                                sh_degree, sh_count, sh.data_ptr(), xy.data_ptr(), z.data_ptr(),
+                                                conic.data_ptr(), ell.data_ptr(), n, img.data_ptr(),
+                                                ranges.data_ptr(), keys[0].data_ptr(), keys[1].data_ptr(),
+                                                vals[0].data_ptr(), vals[1].data_ptr(), cap, 148 * 8, ms,
+                                                ctypes.byref(fms), ctypes.byref(sel))
+                if k >= cap:
+                    break
+                if f >= warmup:
+                    times.append(fms.value)
+                    stage.append(list(ms))
+            if k < cap:
+                break
+            cap *= 2  # saturated: the reference doubles its lists for the next frame (main.cpp:330-338)
+        return img.cpu().numpy(), int(k), times, np.mean(np.array(stage), 0).tolist()
 
     @staticmethod
     def camera56(cam) -> np.ndarray:

@@ -669,6 +669,43 @@ void gso_ranges(int64_t k, const uint64_t* keys, int32_t num_tiles, int32_t* ran
     }
 }
 
+/* ---- camera ---------------------------------------------------------------- */
+
+/* Look-at camera: glm::lookAtRH (external/glm/glm/ext/matrix_transform.inl:
+ * 99-119) for the view matrix, core/camera.cpp:30-55 for the pose, and the
+ * built frame loop's projection terms (app/main.cpp:352-358):
+ * cot_y = 1/tan(fovy/2), cot_x = cot_y/aspect, depth (-2/(f-n), -(f+n)/(f-n)). */
+void gso_look_at(gso_camera* cam, const float eye[3], const float target[3], const float up[3], float fovy_rad,
+                 int32_t width, int32_t height, float znear, float zfar)
+{
+    float f[3] = {target[0] - eye[0], target[1] - eye[1], target[2] - eye[2]};
+    const float fl = 1.0f / sqrtf(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    for (int k = 0; k < 3; ++k) f[k] *= fl;
+    float s[3] = {f[1] * up[2] - f[2] * up[1], f[2] * up[0] - f[0] * up[2], f[0] * up[1] - f[1] * up[0]};
+    const float sl = 1.0f / sqrtf(s[0] * s[0] + s[1] * s[1] + s[2] * s[2]);
+    for (int k = 0; k < 3; ++k) s[k] *= sl;
+    const float u[3] = {s[1] * f[2] - s[2] * f[1], s[2] * f[0] - s[0] * f[2], s[0] * f[1] - s[1] * f[0]};
+    float* m = cam->view;
+    memset(m, 0, sizeof(cam->view));
+    /* column-major: m[col * 4 + row] */
+    m[0] = s[0]; m[4] = s[1]; m[8] = s[2];
+    m[1] = u[0]; m[5] = u[1]; m[9] = u[2];
+    m[2] = -f[0]; m[6] = -f[1]; m[10] = -f[2];
+    m[12] = -(s[0] * eye[0] + s[1] * eye[1] + s[2] * eye[2]);
+    m[13] = -(u[0] * eye[0] + u[1] * eye[1] + u[2] * eye[2]);
+    m[14] = (f[0] * eye[0] + f[1] * eye[1] + f[2] * eye[2]);
+    m[15] = 1.0f;
+    for (int k = 0; k < 3; ++k) cam->position[k] = eye[k];
+    cam->width = width;
+    cam->height = height;
+    cam->aspect = (float)width / (float)height;
+    const float coty = 1.0f / tanf(fovy_rad * 0.5f);
+    cam->fov_cotangent[0] = coty / cam->aspect;
+    cam->fov_cotangent[1] = coty;
+    cam->depth_scale_bias[0] = -2.0f / (zfar - znear);
+    cam->depth_scale_bias[1] = -(zfar + znear) / (zfar - znear);
+}
+
 /* ---- raster (core/gaussian_render.cu:679-759) ----------------------------- */
 
 /* Work count of the GPU's T_min raster, which has no counterpart in the

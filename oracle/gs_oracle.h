@@ -48,6 +48,11 @@ typedef struct gso_cfg {
     int32_t tile_w, tile_h;
 } gso_cfg;
 
+/* Look-at camera (glm::lookAtRH view, core/camera.cpp:30-55 pose, the built
+ * frame loop's projection terms app/main.cpp:352-358); fovy in radians. */
+void gso_look_at(gso_camera* cam, const float eye[3], const float target[3], const float up[3], float fovy_rad,
+                 int32_t width, int32_t height, float znear, float zfar);
+
 /* 0: no contraction; 1: fuse the first product of a sum; 2: fuse the last. */
 void gso_set_fma_mode(int mode);
 /* float -> uint8 conversion of the final colour: 0 saturate, 1 int32 low byte,

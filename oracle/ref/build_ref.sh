@@ -18,9 +18,13 @@
 #      `glm::vec3(splatColor)`.
 # None of the edits touches an arithmetic expression.
 #
-# Usage: build_ref.sh <reference-root> <repo-root>
+# Usage: build_ref.sh <reference-root> [<repo-root>]
 set -euo pipefail
-REF=${1:-/root/reference}
+if [ $# -lt 1 ]; then
+  echo "usage: build_ref.sh <reference-root> [<repo-root>]" >&2
+  exit 2
+fi
+REF=$1
 REPO=${2:-$(cd "$(dirname "$0")/../.." && pwd)}
 OUT="$REPO/oracle/_ref"
 if [ ! -f "$REF/core/gaussian_render.cu" ]; then
@@ -50,6 +54,20 @@ nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -lineinfo \
   -diag-suppress 20012,20014,20011,20013,177,550,2361,3012,1444 \
   "$TMP/ref_harness.cu" -o "$OUT/libgsref.so"
 echo "build_ref: wrote $OUT/libgsref.so"
+
+# The same harness with the stage functions of include/gs_stage_compat.hpp
+# (gs_b200 behind the reference's declarations) in place of the reference's
+# kernels: the stage-API drop-in test.  Links the product library.
+if [ -f "$REPO/3dgaussianrenderer_b200/libgs_b200.so" ]; then
+  nvcc -std=c++17 -O3 -gencode arch=compute_100a,code=sm_100a -lineinfo \
+    -Xcompiler -fPIC -shared -DGS_HARNESS_STAGE_COMPAT \
+    -I"$TMP" -I"$REPO/oracle/ref" -I"$REPO/include" -I"$REF/external/glm" \
+    -include cstdio -include cassert -include cstdlib \
+    -diag-suppress 20012,20014,20011,20013,177,550,2361,3012,1444 \
+    "$TMP/ref_harness.cu" -o "$OUT/libgscompat.so" \
+    -L"$REPO/3dgaussianrenderer_b200" -lgs_b200 -Xlinker -rpath -Xlinker '$ORIGIN/../../3dgaussianrenderer_b200'
+  echo "build_ref: wrote $OUT/libgscompat.so"
+fi
 
 # parsePly compiles as it lies (plain C++; glm and CUDA's vector_types.h);
 # -ffp-contract=off keeps its float arithmetic uncontracted, as MSVC's

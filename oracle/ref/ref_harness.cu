@@ -7,6 +7,14 @@
 // timing load it to obtain the reference's outputs and frame times on the
 // same B200 and the same inputs.
 //
+// Built a second time with GS_HARNESS_STAGE_COMPAT defined (into
+// oracle/_ref/libgscompat.so), the same frame loop calls the same eight
+// stage functions declared by the reference's own gaussian_render.cuh, but
+// implemented by include/gs_stage_compat.hpp on gs_b200 instead of by
+// core/gaussian_render.cu: the drop-in test of the stage API, which shows a
+// program written against the reference rendering through gs_b200
+// unchanged.  The device-helper probes exist only in the reference build.
+//
 // It reproduces the headless part of the reference frame loop
 // (app/main.cpp:360-432): clear the colour buffer and tile ranges, upload
 // GlobalArgs/TileListArgs to constant memory, then SH -> project -> build ->
@@ -15,7 +23,12 @@
 // helpers (core/gaussian_render.cu:234-310) on caller-supplied inputs so the
 // CPU oracle's float semantics can be pinned against them.
 
-#include "gaussian_render.cu"  // patched copy produced by build_ref.sh
+#ifdef GS_HARNESS_STAGE_COMPAT
+#include "gaussian_render.cuh"     // the reference's declarations (patched copy produced by build_ref.sh)
+#include "gs_stage_compat.hpp"     // ... implemented on gs_b200
+#else
+#include "gaussian_render.cu"      // patched copy produced by build_ref.sh
+#endif
 
 #include <cstring>
 
@@ -218,6 +231,7 @@ int gsref_tile_size()
     return k_TileSize;
 }
 
+#ifndef GS_HARNESS_STAGE_COMPAT
 // ---- probes of the reference's device helpers ------------------------------
 
 // ell: n x 6 floats (centre.x, centre.y, cos, sin, extent.x, extent.y)
@@ -282,5 +296,7 @@ int gsref_probe_key(int n, const void* tile, const void* depth, void* out)
                                                    (unsigned long long*) out);
     return (int) cudaDeviceSynchronize();
 }
+
+#endif  // GS_HARNESS_STAGE_COMPAT
 
 }  // extern "C"

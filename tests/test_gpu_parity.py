@@ -75,14 +75,13 @@ def test_project_vs_reference(gs, name):
     xy, z, ell, con = (t.cpu().numpy() for t in project_gpu(gs, d["pos4"], d["sr4"], cam))
     vis = d["ref_ell"][:, 2] > 0
     assert np.array_equal(ell[:, 2] > 0, vis)
-    np.testing.assert_allclose(z, d["ref_z"], rtol=DEPTH_RTOL, atol=1e-7)
-    np.testing.assert_allclose(xy[vis], d["ref_xy"][vis], rtol=1e-6, atol=1e-7)
-    np.testing.assert_allclose(ell[vis], d["ref_ell"][vis], rtol=1e-5, atol=1e-6)
-    np.testing.assert_allclose(con[vis, :3], d["ref_conic"][vis, :3], rtol=1e-4, atol=1e-3)
-    # report bit-exactness of every projected float
-    exact = {k: float(bits_equal(a, d["ref_" + k]).mean()) for k, a in
-             (("xy", xy), ("z", z), ("ell", ell), ("conic", con))}
-    print(name, "bit-exact fraction", exact)
+    # every projected float of every splat, culled ones included, is the
+    # reference's bit for bit (the depth bar of 1e-6 relative holds a fortiori)
+    for k, a in (("xy", xy), ("z", z), ("ell", ell), ("conic", con[:, :3])):
+        ref = d["ref_" + k] if k != "conic" else d["ref_conic"][:, :3]
+        eq = bits_equal(a, ref) | (np.isnan(a) & np.isnan(ref))
+        assert eq.all(), f"{name}: {k} differs from the reference at {np.count_nonzero(~eq)} values"
+    np.testing.assert_allclose(z, d["ref_z"], rtol=DEPTH_RTOL, atol=0)
 
 
 @pytest.mark.parametrize("name", golden_frames())
@@ -96,6 +95,26 @@ def test_sh_vs_reference(gs, name):
     col = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
     gs.stage_sh(n, dev(d["pos4"]), dev(gs.scenes.grouped_sh(d["sh"])), 3 * (deg + 1) ** 2, min(deg, 2), cam, col)
     np.testing.assert_allclose(col.cpu().numpy(), d["ref_color"], atol=1e-6)
+
+
+@pytest.mark.parametrize("deg", [1, 2, 3])
+def test_sh_stage_vs_oracle(gs, O, deg):
+    """SH colour of gs_stage_sh against the oracle at each degree, degree 3
+    included (its terms follow cuda_renderer.cu:119-156; the reference's
+    built kernel stops at degree 2, gaussian_render.cu:62-91)."""
+    sc = gs.scenes.uniform_scene(50_000, seed=40 + deg, sh_degree=3)
+    sh = gs.scenes.grouped_sh(sc["sh"])
+    cam = gs.look_at((0.4, -0.3, 2.5), (0, 0, 0), (0, 1, 0), 60.0, 800, 800, 0.1, 100.0)
+    n = sc["pos4"].shape[0]
+    col = torch.zeros((n, 4), dtype=torch.float32, device="cuda")
+    gs.stage_sh(n, dev(sc["pos4"]), dev(sh), 48, deg, cam, col)
+    got = col.cpu().numpy()
+    want = O.sh(sc["pos4"], sh, 48, deg, np.array(cam.GetPosition(), np.float32))
+    np.testing.assert_allclose(got, want, atol=1e-6, rtol=0)
+    if deg == 3:
+        # the degree-3 terms are large enough to matter in this scene
+        lower = O.sh(sc["pos4"], sh, 48, 2, np.array(cam.GetPosition(), np.float32))
+        assert np.abs(want[:, :3] - lower[:, :3]).max() > 1e-3
 
 
 @pytest.mark.parametrize("name", golden_frames())

@@ -240,3 +240,20 @@ def test_block_eval_count_of_the_warp_culled_raster(O, gs):
     O.render(sc, sh, cam, gs.RenderConfig.reference())
     assert O.block_evals() == 0
     O.count_block_evals(False)
+
+
+def test_oracle_camera_equals_product_camera(O, gs):
+    """The oracle's own look-at camera (used where the product library must
+    not be loaded, e.g. the reference arm of bench.py) is the product's
+    gs_camera_look_at bit for bit."""
+    import ctypes
+    rng = np.random.default_rng(8)
+    poses = [((0.0, 0.0, 3.0), 60.0, 800, 800), ((0.2, 0.1, 3.0), 60.0, 320, 240)]
+    poses += [(tuple(gs.scenes.sphere_pose(rng, r)), 50.0, w, h) for r, (w, h) in
+              zip((10.0, 12.0, 15.0), ((1920, 1080), (1280, 720), (1024, 1024)))]
+    poses += [(tuple(e), 50.0, 1600, 900) for e in gs.scenes.orbit_ring(4, 15.0, seed=1000)]
+    for eye, fovy, W, H in poses:
+        a = gs.look_at(eye, (0, 0, 0), (0, 1, 0), fovy, W, H, 0.1, 100.0)
+        b = O.look_at(eye, (0, 0, 0), (0, 1, 0), fovy, W, H, 0.1, 100.0)
+        assert bytes(a.c) == bytes(b), (eye, fovy, W, H)
+        assert ctypes.sizeof(b) == ctypes.sizeof(a.c)

@@ -61,6 +61,10 @@ def test_sort_noalloc_matches_sort_two_calls_in_a_row(gs):
     f = _noalloc(gs)
     ctx = gs.Context(0)
     cases = [(1_000_003, 44, 1), (gs.lib.gs_stage_sort_noalloc_max_keys(), 51, 2)]
+    # a first tiny call loads the library's kernels (lazy module loading may
+    # take device memory once); the measured calls after it must take none
+    wk, wv = _keys(1, 44, 0)
+    _sort_noalloc(f, wk, wv, 44)
     consumed = []
     for n, bits, seed in cases:
         keys, vals = _keys(n, bits, seed)
@@ -72,9 +76,40 @@ def test_sort_noalloc_matches_sort_two_calls_in_a_row(gs):
         order = np.argsort(keys, kind="stable")
         assert np.array_equal(got_k, keys[order]) and np.array_equal(got_v, vals[order])
         consumed.append(used)
-    # the second call runs only already-loaded kernels: no device memory may move
-    assert consumed[1] == 0
+    # both calls run only already-loaded kernels: no device memory may move
+    assert consumed == [0, 0]
     ctx.close()
+
+
+def test_sort_noalloc_across_the_epoch_wrap(gs):
+    """The look-back words are tagged with a 16-bit epoch that advances by
+    one per pass; after about 0xFFFF / 8 calls of 64-bit keys it wraps and
+    the words are cleared once.  Calls on both sides of the wrap sort
+    exactly like numpy's stable sort."""
+    f = _noalloc(gs)
+    n, bits = 3000, 64
+    rng = np.random.default_rng(9)
+    keys = rng.integers(0, 2 ** 63, n, dtype=np.uint64) * np.uint64(2)
+    keys[::7] = keys[0]  # equal keys: the order of their values is checked too
+    vals = rng.permutation(n).astype(np.int32)
+    order = np.argsort(keys, kind="stable")
+    k = torch.from_numpy(keys.view(np.int64).copy()).cuda()
+    v = torch.from_numpy(vals.copy()).cuda()
+    ka, va = torch.empty_like(k), torch.empty_like(v)
+    sel = ctypes.c_int32(-1)
+    calls = 0xFFFF // 8 + 3
+    checked = 0
+    for i in range(calls):
+        k.copy_(torch.from_numpy(keys.view(np.int64)))
+        v.copy_(torch.from_numpy(vals))
+        assert f(n, bits, k.data_ptr(), v.data_ptr(), ka.data_ptr(), va.data_ptr(), ctypes.byref(sel), None) == 0
+        if i < 2 or i >= calls - 4:
+            out_k = (ka if sel.value else k).cpu().numpy().view(np.uint64)
+            out_v = (va if sel.value else v).cpu().numpy()
+            assert np.array_equal(out_k, keys[order]), i
+            assert np.array_equal(out_v, vals[order]), i
+            checked += 1
+    assert checked == 6
 
 
 def test_sort_noalloc_rejects_more_than_its_limit(gs):
