@@ -41,6 +41,7 @@ GS_TERM_REFERENCE = 0
 GS_TERM_TMIN = 1
 GS_ORDER_BUCKETS = 0
 GS_ORDER_ONESWEEP = 1
+GS_ORDER_AUTO = 2
 GS_SCENE_KEEP_ORDER = 1
 
 
@@ -75,6 +76,9 @@ class gs_render_cfg(ctypes.Structure):
         ("sort_variant", ctypes.c_int32),
         ("views_per_block", ctypes.c_int32),
         ("graph", ctypes.c_int32),
+        ("raster_chunk", ctypes.c_int32),
+        ("raster_persistent", ctypes.c_int32),
+        ("sort_bits", ctypes.c_int32),
     ]
 
 
@@ -297,6 +301,9 @@ class RenderConfig:
     sort_variant: int = 0
     views_per_block: int = 0
     graph: int = 1
+    raster_chunk: int = 0       # T_min raster: Gaussians per shared-memory batch (0 = 32, or 64)
+    raster_persistent: int = 0  # T_min raster: persistent CTAs over the atomic tile queue
+    sort_bits: int = 0          # per-tile sort: radix-sorted top depth bits (0 = 16, 8..32)
 
     @staticmethod
     def reference() -> "RenderConfig":
@@ -304,7 +311,8 @@ class RenderConfig:
 
     def c(self) -> gs_render_cfg:
         return gs_render_cfg(self.sh_max_degree, self.termination, self.t_min, self.tile_w, self.tile_h,
-                             self.ordering, self.sort_variant, self.views_per_block, self.graph)
+                             self.ordering, self.sort_variant, self.views_per_block, self.graph, self.raster_chunk,
+                             self.raster_persistent, self.sort_bits)
 
 
 def num_tiles(width: int, height: int, cfg: RenderConfig) -> int:
@@ -452,7 +460,7 @@ def probe_tile_lists(ctx: Context) -> dict:
 
 def _from_c(c: gs_render_cfg) -> "RenderConfig":
     return RenderConfig(c.sh_max_degree, c.termination, c.t_min, c.tile_w, c.tile_h, c.ordering, c.sort_variant,
-                        c.views_per_block, c.graph)
+                        c.views_per_block, c.graph, c.raster_chunk, c.raster_persistent, c.sort_bits)
 
 
 def autotune(ctx: Context, scene: Scene, cams: list, cfg: RenderConfig, iterations: int = 5, stream=None):

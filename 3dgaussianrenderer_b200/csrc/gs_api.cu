@@ -162,6 +162,7 @@ struct HostCopy {
 struct TuneEntry {
     int32_t n_log2 = 0, px_log2 = 0, views_bucket = 0, termination = 0, ordering = 0;
     int32_t tile_w = 16, tile_h = 16, views_per_block = 0, sort_variant = 0;
+    int32_t ordering_picked = 0, raster_chunk = 0, raster_persistent = 0, sort_bits = 0;
     double ms = 0.0;
     uint64_t stamp = 0;  // insertion order: the oldest entry goes when the table is full
 };
@@ -275,7 +276,10 @@ bool valid_cfg(const gs_render_cfg& c)
                        (c.tile_w == 8 && c.tile_h == 8);
     return shape && c.sh_max_degree >= 0 && c.sh_max_degree <= 3 && c.sort_variant >= 0 &&
            c.sort_variant < kSortVariants && c.views_per_block >= 0 &&
-           (c.ordering == GS_ORDER_BUCKETS || c.ordering == GS_ORDER_ONESWEEP) && (c.graph == 0 || c.graph == 1) &&
+           (c.ordering == GS_ORDER_BUCKETS || c.ordering == GS_ORDER_ONESWEEP || c.ordering == GS_ORDER_AUTO) &&
+           (c.graph == 0 || c.graph == 1) && (c.raster_chunk == 0 || c.raster_chunk == 32 || c.raster_chunk == 64) &&
+           (c.raster_persistent == 0 || c.raster_persistent == 1) &&
+           (c.sort_bits == 0 || (c.sort_bits >= 8 && c.sort_bits <= 32)) &&
            (c.termination == GS_TERM_REFERENCE || c.termination == GS_TERM_TMIN);
 }
 
@@ -526,6 +530,8 @@ int run_frame_onesweep(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams
     ra.rec = cfg.termination == GS_TERM_TMIN ? ctx->rec.as<float4>() : nullptr;
     ra.t_min = cfg.t_min;
     ra.tile_counter = &dc->raster_tile;
+    ra.rec_chunk = cfg.raster_chunk;
+    ra.rec_persistent = cfg.raster_persistent;
     launch_raster(ra, cfg.tile_w, cfg.tile_h, cfg.termination, num_views > 1, ctx->num_sms, st);
     GS_CUDA(cudaGetLastError());
     GS_CUDA(cudaEventRecord(ctx->ev[5], st));
@@ -721,6 +727,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     sa.slot_gi = ctx->offsets.as<int32_t>();
     sa.big_list = ctx->big_list.as<int32_t>();
     sa.big_count = &dc->big_tiles;
+    sa.prefix_bits = cfg.sort_bits;
     if (p.n > 0) launch_tile_sort(sa, ctx->num_sms, st);
     GS_CUDA(record(ctx->ev[4], st, capturing));
 
@@ -742,6 +749,9 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ra.slot_gi = ctx->offsets.as<int32_t>();
     ra.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     ra.order = ctx->tile_order.as<int32_t>();
+    ra.rec_chunk = cfg.raster_chunk;
+    ra.rec_persistent = cfg.raster_persistent;
+    ra.sort_prefix_bits = cfg.sort_bits;
     if (p.host_copy && p.host_copy->groups > 1 && ra.rec) {
         // one launch per view group, in view order; a group's images are
         // complete at its event
@@ -754,6 +764,8 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
             RasterArgs rg = ra;
             rg.tile_base = t0;
             rg.num_tiles_total = t1 - t0;
+            // a persistent group launch starts its own queue from zero
+            if (rg.rec_persistent) GS_CUDA(cudaMemsetAsync(&dc->raster_tile, 0, sizeof(unsigned long long), st));
             launch_raster(rg, cfg.tile_w, cfg.tile_h, cfg.termination, false, ctx->num_sms, st);
             GS_CUDA(record(ctx->ev_group[g], st, capturing));
         }
@@ -978,9 +990,11 @@ int run_frame_halves(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
     return GS_OK;
 }
 
-int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg,
+int run_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int num_views, const gs_render_cfg& cfg_in,
               uint8_t* const* outs, gs_stats* stats, cudaStream_t st)
 {
+    gs_render_cfg cfg = cfg_in;
+    if (cfg.ordering == GS_ORDER_AUTO) cfg.ordering = GS_ORDER_BUCKETS;  // not tuned: the default ordering
     if (num_views > 1 && scene && scene->n * (int64_t)num_views >= (1ll << 31))
         return run_frame_halves(ctx, scene, cams, num_views, cfg, outs, stats, st, 0);
     int rc;
@@ -1025,46 +1039,60 @@ bool same_bucket(const TuneEntry& a, const TuneEntry& b)
            a.termination == b.termination && a.ordering == b.ordering;
 }
 
-// The knob settings gs_autotune times: tile shapes only where the images do
-// not depend on them (per-pixel termination), views per block only where
-// they change the frame kernel's grouping (distinct min(V, vpb)), onesweep
-// tile shapes only for onesweep frames.
-std::vector<gs_render_cfg> tune_candidates(const gs_render_cfg& base, int num_views)
+// One knob of gs_autotune's coordinate descent: its values, and how a value
+// is written into a configuration.
+struct TuneKnob {
+    std::vector<int> values;
+    void (*apply)(gs_render_cfg&, int);
+};
+
+// The knobs gs_autotune sweeps for `base` and `num_views`, in sweep order:
+// tile shapes only where the images do not depend on them (per-pixel
+// termination), views per block only where they change the frame kernel's
+// grouping (distinct min(V, vpb)), the ordering only when base asks for
+// GS_ORDER_AUTO, the onesweep tile shape for onesweep frames, the tile sort's
+// radix width for bucket frames, the record raster's knobs for T_min frames.
+// Knobs whose relevance depends on the ordering are listed after it and
+// skipped when the ordering picked so far does not use them.
+std::vector<TuneKnob> tune_knobs(const gs_render_cfg& base, int num_views)
 {
-    static const int kShapes[3][2] = {{16, 16}, {16, 8}, {8, 8}};
-    std::vector<std::pair<int, int>> shapes;
+    std::vector<TuneKnob> k;
     if (base.termination == GS_TERM_TMIN)
-        for (const auto& s : kShapes) shapes.emplace_back(s[0], s[1]);
-    else
-        shapes.emplace_back(base.tile_w, base.tile_h);
-    std::vector<int> vpbs;
+        k.push_back({{0, 1, 2}, [](gs_render_cfg& c, int v) {
+                         static const int shapes[3][2] = {{16, 16}, {16, 8}, {8, 8}};
+                         c.tile_w = shapes[v][0];
+                         c.tile_h = shapes[v][1];
+                     }});
     if (num_views > 8) {
+        std::vector<int> vpbs;
         int last = 0;
         for (int v : {8, 16, 32}) {
             const int eff = std::min(num_views, v);
             if (eff != last) vpbs.push_back(v);
             last = eff;
         }
-    } else {
-        vpbs.push_back(base.views_per_block);
+        k.push_back({vpbs, [](gs_render_cfg& c, int v) { c.views_per_block = v; }});
     }
-    std::vector<int> variants;
-    if (base.ordering == GS_ORDER_ONESWEEP)
-        for (int v = 0; v < kSortVariants; ++v) variants.push_back(v);
-    else
-        variants.push_back(base.sort_variant);
-    std::vector<gs_render_cfg> out;
-    for (const auto& s : shapes)
-        for (int vpb : vpbs)
-            for (int sv : variants) {
-                gs_render_cfg c = base;
-                c.tile_w = s.first;
-                c.tile_h = s.second;
-                c.views_per_block = vpb;
-                c.sort_variant = sv;
-                out.push_back(c);
-            }
-    return out;
+    if (base.ordering == GS_ORDER_AUTO)
+        k.push_back({{GS_ORDER_BUCKETS, GS_ORDER_ONESWEEP}, [](gs_render_cfg& c, int v) { c.ordering = v; }});
+    k.push_back({{0, 1, 2, 3}, [](gs_render_cfg& c, int v) { c.sort_variant = v; }});
+    k.push_back({{8, 16, 24, 32}, [](gs_render_cfg& c, int v) { c.sort_bits = v; }});
+    if (base.termination == GS_TERM_TMIN) {
+        k.push_back({{32, 64}, [](gs_render_cfg& c, int v) { c.raster_chunk = v; }});
+        k.push_back({{0, 1}, [](gs_render_cfg& c, int v) { c.raster_persistent = v; }});
+    }
+    return k;
+}
+
+// Whether a knob (by its setter) matters for the configuration as tuned so far.
+bool knob_applies(const TuneKnob& k, const gs_render_cfg& c)
+{
+    gs_render_cfg a = c, b = c;
+    k.apply(a, k.values.front());
+    k.apply(b, k.values.back());
+    if (a.sort_variant != b.sort_variant) return c.ordering == GS_ORDER_ONESWEEP;
+    if (a.sort_bits != b.sort_bits) return c.ordering != GS_ORDER_ONESWEEP;
+    return true;
 }
 
 }  // namespace
@@ -1106,6 +1134,9 @@ void gs_default_cfg(gs_render_cfg* cfg)
     cfg->sort_variant = 0;
     cfg->views_per_block = 0;
     cfg->graph = 1;
+    cfg->raster_chunk = 0;
+    cfg->raster_persistent = 0;
+    cfg->sort_bits = 0;
 }
 
 void gs_camera_look_at(gs_camera* cam, const float eye[3], const float target[3], const float up[3], float fovy_rad,
@@ -1439,7 +1470,7 @@ int gs_render_batch_host(gs_ctx* ctx, const gs_scene* scene, const gs_camera* ca
         return GS_OK;
     }
     if (!ctx->copy_stream) GS_CUDA(cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking));
-    if (cfg->ordering == GS_ORDER_BUCKETS && cfg->termination == GS_TERM_TMIN) {
+    if ((cfg->ordering == GS_ORDER_BUCKETS || cfg->ordering == GS_ORDER_AUTO) && cfg->termination == GS_TERM_TMIN) {
         // one frame for all views; its raster runs in view groups, each
         // group read back on the copy stream while the next one renders
         HostCopy hc;
@@ -1711,14 +1742,19 @@ int gs_autotune(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32
         return cuda_fail(cudaGetLastError(), "tuning events");
     }
 
-    const std::vector<gs_render_cfg> cands = tune_candidates(*base, num_views);
-    int rc = GS_OK, timed = 0, win = -1;
-    double win_ms = 0.0;
-    std::vector<float> times((size_t)iterations);
-    for (size_t i = 0; i < cands.size() && rc == GS_OK; ++i) {
-        const gs_render_cfg& c = cands[i];
+    // coordinate descent: each knob at all its values, the others at the
+    // best so far; a candidate already timed is not timed again
+    std::vector<gs_render_cfg> timed_cfgs;
+    std::vector<double> timed_ms;
+    auto time_cfg = [&](const gs_render_cfg& c, double& ms) -> int {
+        for (size_t i = 0; i < timed_cfgs.size(); ++i)
+            if (std::memcmp(&timed_cfgs[i], &c, sizeof(c)) == 0) {
+                ms = timed_ms[i];
+                return GS_OK;
+            }
         int r = GS_OK;
         for (int w = 0; w < 2 && r == GS_OK; ++w) r = run_frame(ctx, scene, cams, num_views, c, outs.data(), nullptr, st);
+        std::vector<float> times((size_t)iterations);
         for (int it = 0; it < iterations && r == GS_OK; ++it) {
             cudaEventRecord(e0, st);
             r = run_frame(ctx, scene, cams, num_views, c, outs.data(), nullptr, st);
@@ -1726,29 +1762,71 @@ int gs_autotune(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32
             if (r == GS_OK && cudaEventSynchronize(e1) != cudaSuccess) r = cuda_fail(cudaGetLastError(), "tuning");
             times[it] = ms_between(e0, e1);
         }
-        if (r == GS_OK) {
-            std::sort(times.begin(), times.end());
-            const double ms = times[(size_t)iterations / 2];
-            if (timed < results_capacity) results[timed] = gs_tune_result{c, ms};
-            ++timed;
-            if (win < 0 || ms < win_ms) win = (int)i, win_ms = ms;
-        } else if (r == GS_ERR_OOM || r == GS_ERR_CAPACITY) {
-            cudaGetLastError();  // this setting does not fit: the others may
-        } else {
-            rc = r;
+        if (r != GS_OK) return r;
+        std::sort(times.begin(), times.end());
+        ms = times[(size_t)iterations / 2];
+        timed_cfgs.push_back(c);
+        timed_ms.push_back(ms);
+        return GS_OK;
+    };
+    gs_render_cfg cur = *base;
+    // defaults spelled out, so a default and its explicit value are one candidate
+    if (cur.ordering == GS_ORDER_AUTO) cur.ordering = GS_ORDER_BUCKETS;
+    if (cur.raster_chunk == 0) cur.raster_chunk = 32;
+    if (cur.sort_bits == 0) cur.sort_bits = 16;
+    int rc = GS_OK;
+    bool have = false;
+    double win_ms = 0.0;
+    for (const TuneKnob& k : tune_knobs(*base, num_views)) {
+        if (rc != GS_OK) break;
+        if (!knob_applies(k, cur)) continue;
+        gs_render_cfg knob_best = cur;
+        for (int v : k.values) {
+            gs_render_cfg c = cur;
+            k.apply(c, v);
+            double ms = 0.0;
+            const int r = time_cfg(c, ms);
+            if (r == GS_OK) {
+                if (!have || ms < win_ms) {
+                    win_ms = ms;
+                    knob_best = c;
+                    have = true;
+                }
+            } else if (r == GS_ERR_OOM || r == GS_ERR_CAPACITY) {
+                cudaGetLastError();  // this setting does not fit: the others may
+            } else {
+                rc = r;
+                break;
+            }
+        }
+        cur = knob_best;
+    }
+    if (!have && rc == GS_OK) {
+        // no knob applies (a single-view reference frame): time the base alone
+        double ms = 0.0;
+        rc = time_cfg(cur, ms);
+        if (rc == GS_OK) {
+            win_ms = ms;
+            have = true;
         }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    const int timed = (int)timed_cfgs.size();
+    for (int i = 0; i < timed && i < results_capacity; ++i) results[i] = gs_tune_result{timed_cfgs[i], timed_ms[i]};
     if (num_results) *num_results = timed;
     if (rc) return rc;
-    if (win < 0) return fail(GS_ERR_OOM, "no knob setting fit in device memory");
+    if (!have) return fail(GS_ERR_OOM, "no knob setting fit in device memory");
 
     TuneEntry e = tune_key(scene->n, pixels, num_views, *base);
-    e.tile_w = cands[win].tile_w;
-    e.tile_h = cands[win].tile_h;
-    e.views_per_block = cands[win].views_per_block;
-    e.sort_variant = cands[win].sort_variant;
+    e.tile_w = cur.tile_w;
+    e.tile_h = cur.tile_h;
+    e.views_per_block = cur.views_per_block;
+    e.sort_variant = cur.sort_variant;
+    e.ordering_picked = cur.ordering;
+    e.raster_chunk = cur.raster_chunk;
+    e.raster_persistent = cur.raster_persistent;
+    e.sort_bits = cur.sort_bits;
     e.ms = win_ms;
     e.stamp = ++ctx->tune_clock;
     auto it = std::find_if(ctx->tune.begin(), ctx->tune.end(), [&](const TuneEntry& x) { return same_bucket(x, e); });
@@ -1760,7 +1838,7 @@ int gs_autotune(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32
                                              [](const TuneEntry& a, const TuneEntry& b) { return a.stamp < b.stamp; }));
         ctx->tune.push_back(e);
     }
-    *best = cands[win];
+    *best = cur;
     if (best_ms) *best_ms = win_ms;
     return GS_OK;
 }
@@ -1779,6 +1857,10 @@ int gs_autotune_lookup(gs_ctx* ctx, int64_t n, int32_t width, int32_t height, in
             cfg->tile_h = e.tile_h;
             cfg->views_per_block = e.views_per_block;
             cfg->sort_variant = e.sort_variant;
+            cfg->ordering = e.ordering_picked;
+            cfg->raster_chunk = e.raster_chunk;
+            cfg->raster_persistent = e.raster_persistent;
+            cfg->sort_bits = e.sort_bits;
             *found = 1;
             break;
         }
@@ -1859,7 +1941,7 @@ int gs_probe_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, in
     if (!ctx || !scene || !cams || !cfg || !d_rgba || !probe || num_views <= 0) return fail(GS_ERR_INVALID, "null argument");
     if (!probe->d_xy || !probe->d_z || !probe->d_ellipse || !probe->d_conic)
         return fail(GS_ERR_INVALID, "probe geometry outputs are required");
-    if (cfg->ordering != GS_ORDER_BUCKETS) return fail(GS_ERR_INVALID, "the probe covers GS_ORDER_BUCKETS frames");
+    if (cfg->ordering == GS_ORDER_ONESWEEP) return fail(GS_ERR_INVALID, "the probe covers GS_ORDER_BUCKETS frames");
     std::lock_guard<std::mutex> lock(ctx->mu);
     gs_render_cfg c = *cfg;
     c.graph = 0;  // the probe outputs are arguments of this launch only

@@ -439,32 +439,37 @@ __device__ void sort_tile_global(const TileSortArgs& a, const int64_t start, con
         }
     };
 
-    run_passes(vary_of(0xFFFFFFFF00000000ull));
-    bool t = false;
-    for (int p = threadIdx.x + 1; p < m; p += NT) t |= (bk[cur][p] >> 32) == (bk[cur][p - 1] >> 32);
-    if (__syncthreads_or(t)) {
-        for (int p = threadIdx.x; p < m; p += NT) {
-            const uint64_t x = bk[cur][p];
-            const int32_t s = have_v ? bv[cur][p] : (int32_t)(uint32_t)x;
-            bv[cur][p] = s;
-            bk[cur][p] = (x & 0xFFFFFFFF00000000ull) | (uint32_t)__ldg(&a.slot_gi[s]);
-        }
-        have_v = true;
-        __syncthreads();
-        run_passes(vary_of(~0ull));
-    }
-    // result into a.vals
-    if (!have_v) {
+    // passes over the top 16 varying depth bits, then the runs of equal
+    // prefixes into (depth, index) order (as in the shared-memory sort); the
+    // keys keep their slots in the low bits throughout
+    int shift;
+    run_passes(tilesort::prefix_window(vary_of(0xFFFFFFFF00000000ull), a.prefix_bits, &shift));
+    bool too_long = false;
+    for (int p = threadIdx.x; p < m; p += NT) too_long |= tilesort::fix_run_at(bk[cur], m, p, shift, a.slot_gi);
+    if (!__syncthreads_or(too_long)) {
+        // result into a.vals
         for (int p = threadIdx.x; p < m; p += NT) bv[0][p] = (int32_t)(uint32_t)bk[cur][p];
-    } else if (cur == 1) {
-        for (int p = threadIdx.x; p < m; p += NT) bv[0][p] = bv[1][p];
+        return;
     }
+    // a long run of equal prefixes: sort again on (depth, index), the slots
+    // carried as values
+    for (int p = threadIdx.x; p < m; p += NT) {
+        const uint64_t x = bk[cur][p];
+        const int32_t s = (int32_t)(uint32_t)x;
+        bv[cur][p] = s;
+        bk[cur][p] = (x & 0xFFFFFFFF00000000ull) | (uint32_t)__ldg(&a.slot_gi[s]);
+    }
+    have_v = true;
+    __syncthreads();
+    run_passes(vary_of(~0ull));
+    if (cur == 1)
+        for (int p = threadIdx.x; p < m; p += NT) bv[0][p] = bv[1][p];
 }
 
 template <int IPT>
 __device__ void sort_big_smem(const TileSortArgs& a, const int64_t start, const int m, const Smem& sm)
 {
-    tilesort::sort_tile<kBigThreads, IPT>(a.keys + start, m, a.slot_gi, sm);
+    tilesort::sort_tile<kBigThreads, IPT>(a.keys + start, m, a.slot_gi, sm, a.prefix_bits);
     for (int p = threadIdx.x; p < m; p += kBigThreads) a.vals[start + p] = (int32_t)(uint32_t)sm.k[p];
 }
 

@@ -176,6 +176,7 @@ struct TileSortArgs {
     const int32_t* slot_gi;
     const int32_t* big_list;         // tiles above the fused capacity (from the tile scan)
     const unsigned int* big_count;
+    int32_t prefix_bits;             // depth bits the radix passes sort (8..32; 0 = 16)
 };
 constexpr int kTileSortSmemKeys = 4096;
 // Keys a tile may have to be sorted inside its raster CTA (TW * TH / 2
@@ -253,6 +254,12 @@ struct RasterArgs {
     const int32_t* slot_gi;
     int32_t fused_cap;
     const int32_t* order;             // non-null: CTA (or queue entry) k rasterises tile order[k]
+    // record raster (GS_TERM_TMIN) knobs: entries culled and staged per warp
+    // step (32 or 64), and a persistent grid over the atomic tile queue
+    // (tile_counter, zero at launch) instead of one CTA per tile
+    int32_t rec_chunk;
+    int32_t rec_persistent;
+    int32_t sort_prefix_bits;         // depth bits the fused tile sort radix-sorts (8..32; 0 = 16)
 };
 
 void launch_sh_stage(int64_t n, const float4* pos, const float* sh, int sh_count, int deg, const ViewParams& v,

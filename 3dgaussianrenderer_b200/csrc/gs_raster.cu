@@ -214,13 +214,13 @@ __device__ __forceinline__ const uint64_t* fused_sort(const RasterArgs& a, const
     sm.run = nullptr;
     const uint64_t* src = a.keys + first;
     if (count <= NT)
-        tilesort::sort_tile<NT, 1>(src, count, a.slot_gi, sm);
+        tilesort::sort_tile<NT, 1>(src, count, a.slot_gi, sm, a.sort_prefix_bits);
     else if (count <= 2 * NT)
-        tilesort::sort_tile<NT, 2>(src, count, a.slot_gi, sm);
+        tilesort::sort_tile<NT, 2>(src, count, a.slot_gi, sm, a.sort_prefix_bits);
     else if (count <= 4 * NT)
-        tilesort::sort_tile<NT, 4>(src, count, a.slot_gi, sm);
+        tilesort::sort_tile<NT, 4>(src, count, a.slot_gi, sm, a.sort_prefix_bits);
     else
-        tilesort::sort_tile<NT, 8>(src, count, a.slot_gi, sm);
+        tilesort::sort_tile<NT, 8>(src, count, a.slot_gi, sm, a.sort_prefix_bits);
     return fs.k;
 }
 
@@ -451,29 +451,43 @@ __device__ __forceinline__ float ex2_approx(const float x)
     return y;
 }
 
-template <int TW, int TH>
-__global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kernel(RasterArgs a)
+// Shared memory of the record raster: per-warp survivor slots (CHUNK per
+// warp) and the fused tile sort.
+template <int TW, int TH, int CHUNK>
+struct RecSmem {
+    static constexpr int NW = TW * TH / 64;
+    float4 s[NW][CHUNK];  // (x, A, B, L)
+    float4 q[NW][CHUNK];  // (y, C, red, green)
+    float b[NW][CHUNK];   // blue
+    FusedSortSmem<TW * TH / 2> fs;
+};
+
+// The view a global tile belongs to: binary search over the views' first tiles.
+__device__ __forceinline__ const ViewParams& view_of_tile(const RasterArgs& a, const int64_t gtile)
 {
-    constexpr int NW = TW * TH / 64;
-    constexpr int WX = TW / 8;
-    __shared__ float4 s_s[NW][32];  // (x, A, B, L)
-    __shared__ float4 s_q[NW][32];  // (y, C, red, green)
-    __shared__ float s_b[NW][32];   // blue
-    __shared__ FusedSortSmem<TW * TH / 2> fs;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : a.tile_base + (int64_t)blockIdx.x;
-    int vi = 0;
-    if (a.num_views > 1) {
-        int hi = a.num_views - 1;
-        while (vi < hi) {
-            const int mid = (vi + hi + 1) >> 1;
-            if (a.views[mid].tile_offset <= gtile)
-                vi = mid;
-            else
-                hi = mid - 1;
-        }
+    if (a.num_views <= 1) return a.view0;
+    int vi = 0, hi = a.num_views - 1;
+    while (vi < hi) {
+        const int mid = (vi + hi + 1) >> 1;
+        if (a.views[mid].tile_offset <= gtile)
+            vi = mid;
+        else
+            hi = mid - 1;
     }
-    const ViewParams& v = a.num_views > 1 ? a.views[vi] : a.view0;
+    return a.views[vi];
+}
+
+// One tile of the record raster.  Every thread of the CTA must call it (the
+// fused sort synchronises the CTA).  CHUNK = the entries a warp culls and
+// stages in shared memory per step, the raster's batch of Gaussians (32 or
+// 64: R = CHUNK / 32 records per lane).
+template <int TW, int TH, int CHUNK>
+__device__ __forceinline__ void raster_rec_tile(const RasterArgs& a, const int64_t gtile, RecSmem<TW, TH, CHUNK>& sm)
+{
+    constexpr int WX = TW / 8;
+    constexpr int R = CHUNK / 32;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const ViewParams& v = view_of_tile(a, gtile);
     const int local_tile = (int)(gtile - v.tile_offset);
     const int first = __ldg(&a.ranges[2 * gtile]);
     const int last = __ldg(&a.ranges[2 * gtile + 1]);
@@ -489,7 +503,7 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
         }
         return;
     }
-    const uint64_t* sk = fused_sort<TW * TH / 2>(a, first, last - first, fs);
+    const uint64_t* sk = fused_sort<TW * TH / 2>(a, first, last - first, sm.fs);
     const float cx = (float)px * v.texel_x - 1.0f;
     const float cy0 = (float)py0 * v.texel_y - 1.0f;
     const float cy1 = (float)py1 * v.texel_y - 1.0f;
@@ -504,43 +518,65 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
 
     // each chunk's cull records are loaded one chunk ahead, so their
     // latency overlaps the blend of the chunk before
-    float4 qn = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4* rpn = nullptr;
-    if (first + lane < last) {
-        rpn = a.rec + 3 * (int64_t)slot_at(a, sk, first, lane);
-        qn = __ldg(rpn);
+    float4 qn[R];
+    const float4* rpn[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        qn[r] = make_float4(0.f, 0.f, 0.f, 0.f);
+        rpn[r] = nullptr;
+        if (first + 32 * r + lane < last) {
+            rpn[r] = a.rec + 3 * (int64_t)slot_at(a, sk, first, 32 * r + lane);
+            qn[r] = __ldg(rpn[r]);
+        }
     }
-    for (int base = first; base < last; base += 32) {
+    for (int base = first; base < last; base += CHUNK) {
         if (__all_sync(kFull, done)) break;
-        const int j = base + lane;
-        bool keep = false;
-        const float4 q0 = qn;  // (x, y, ext_x, ext_y)
-        const float4* rp = rpn;
-        if (j < last)
-            keep = (q0.x - q0.z <= bx1) && (q0.x + q0.z >= bx0) && (q0.y - q0.w <= by1) && (q0.y + q0.w >= by0);
-        const unsigned bal = __ballot_sync(kFull, keep);
-        float4 q1, q2;
-        if (keep) {
-            q1 = __ldg(rp + 1);  // (A, B, C, L)
-            q2 = __ldg(rp + 2);  // (red, green, blue, 0)
+        bool keep[R];
+        unsigned bal[R];
+        const float4* rp[R];
+        float4 q0[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = base + 32 * r + lane;
+            q0[r] = qn[r];  // (x, y, ext_x, ext_y)
+            rp[r] = rpn[r];
+            keep[r] = j < last && (q0[r].x - q0[r].z <= bx1) && (q0[r].x + q0[r].z >= bx0) &&
+                      (q0[r].y - q0[r].w <= by1) && (q0[r].y + q0[r].w >= by0);
+            bal[r] = __ballot_sync(kFull, keep[r]);
         }
-        if (j + 32 < last) {
-            rpn = a.rec + 3 * (int64_t)slot_at(a, sk, first, j + 32 - first);
-            qn = __ldg(rpn);
+        float4 q1[R], q2[R];
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+            if (keep[r]) {
+                q1[r] = __ldg(rp[r] + 1);  // (A, B, C, L)
+                q2[r] = __ldg(rp[r] + 2);  // (red, green, blue, 0)
+            }
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const int j = base + CHUNK + 32 * r + lane;
+            if (j < last) {
+                rpn[r] = a.rec + 3 * (int64_t)slot_at(a, sk, first, j - first);
+                qn[r] = __ldg(rpn[r]);
+            }
         }
-        if (keep) {
-            const int k = __popc(bal & lt);
-            s_s[warp][k] = make_float4(q0.x, q1.x, q1.y, q1.w);
-            s_q[warp][k] = make_float4(q0.y, q1.z, q2.x, q2.y);
-            s_b[warp][k] = q2.z;
+        int below = 0;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            if (keep[r]) {
+                const int k = below + __popc(bal[r] & lt);
+                sm.s[warp][k] = make_float4(q0[r].x, q1[r].x, q1[r].y, q1[r].w);
+                sm.q[warp][k] = make_float4(q0[r].y, q1[r].z, q2[r].x, q2[r].y);
+                sm.b[warp][k] = q2[r].z;
+            }
+            below += __popc(bal[r]);
         }
         __syncwarp();  // slot writes visible to the whole warp
-        const int cnt = __popc(bal);
+        const int cnt = below;
 #pragma unroll 4
         for (int k = 0; k < cnt; ++k) {
-            const float4 e = s_s[warp][k];
-            const float4 q = s_q[warp][k];
-            const float bl = s_b[warp][k];
+            const float4 e = sm.s[warp][k];
+            const float4 q = sm.q[warp][k];
+            const float bl = sm.b[warp][k];
             const float dx = cx - e.x;
             const float adx2 = fmaf(e.y * dx, dx, e.w);  // A dx^2 + L
             const float bdx = __fmul_rn(e.z, dx);  // kept apart from the fma below
@@ -567,11 +603,65 @@ __global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kern
     if (in1) store_pixel(v, px, py1, R1, G1, B1);
 }
 
+// One CTA per tile, in the raster order (heavy tiles first) or of the view
+// group [tile_base, tile_base + grid).
+template <int TW, int TH, int CHUNK>
+__global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_kernel(RasterArgs a)
+{
+    __shared__ RecSmem<TW, TH, CHUNK> sm;
+    const int64_t gtile = a.order ? (int64_t)__ldg(&a.order[blockIdx.x]) : a.tile_base + (int64_t)blockIdx.x;
+    raster_rec_tile<TW, TH, CHUNK>(a, gtile, sm);
+}
+
+// Persistent CTAs (as many as fit on the SMs at once) that pull tiles from
+// an atomic queue over the raster order (heavy tiles first) until it runs
+// dry.
+template <int TW, int TH, int CHUNK>
+__global__ void __launch_bounds__(TW * TH / 2, 2048 / (TW * TH)) raster_rec_persistent_kernel(RasterArgs a)
+{
+    __shared__ RecSmem<TW, TH, CHUNK> sm;
+    __shared__ int64_t s_tile;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const int64_t k = (int64_t)atomicAdd(a.tile_counter, 1ull);
+            s_tile = k < a.num_tiles_total ? (a.order ? (int64_t)__ldg(&a.order[k]) : a.tile_base + k) : -1;
+        }
+        __syncthreads();
+        const int64_t gtile = s_tile;
+        if (gtile < 0) return;
+        raster_rec_tile<TW, TH, CHUNK>(a, gtile, sm);
+        __syncthreads();  // s_tile and the sort's shared memory are reused
+    }
+}
+
+template <int TW, int TH, int CHUNK>
+static void launch_rec(const RasterArgs& a, bool persistent, int num_sms, cudaStream_t st)
+{
+    if (a.num_tiles_total <= 0) return;
+    if (!persistent) {
+        raster_rec_kernel<TW, TH, CHUNK><<<(unsigned)a.num_tiles_total, TW * TH / 2, 0, st>>>(a);
+        return;
+    }
+    static int per_sm = 0;  // same on every B200; queried once
+    if (per_sm == 0) {
+        int x = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&x, raster_rec_persistent_kernel<TW, TH, CHUNK>, TW * TH / 2, 0);
+        per_sm = std::max(x, 1);
+    }
+    const int64_t grid = std::min<int64_t>((int64_t)per_sm * num_sms, a.num_tiles_total);
+    raster_rec_persistent_kernel<TW, TH, CHUNK><<<(unsigned)grid, TW * TH / 2, 0, st>>>(a);
+}
+
 template <int TW, int TH>
 static void launch_shape(const RasterArgs& a, int termination, bool persistent, int num_sms, cudaStream_t st)
 {
     if (a.rec && termination == 1) {
-        if (a.num_tiles_total > 0) raster_rec_kernel<TW, TH><<<(unsigned)a.num_tiles_total, TW * TH / 2, 0, st>>>(a);
+        // the record raster's queue is the frame's tile counter; persistent
+        // only when asked (RasterArgs::rec_persistent)
+        if (a.rec_chunk == 64)
+            launch_rec<TW, TH, 64>(a, a.rec_persistent != 0, num_sms, st);
+        else
+            launch_rec<TW, TH, 32>(a, a.rec_persistent != 0, num_sms, st);
         return;
     }
     if (termination == 0) {

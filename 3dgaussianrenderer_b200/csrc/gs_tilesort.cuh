@@ -7,11 +7,14 @@
 // among equal depths, the (view * n + i) index of the slot -- the order of
 // a stable sort of the reference's (tile | depth) keys emitted in Gaussian
 // order (core/gaussian_render.cu:591-632 sorts with CUB's stable radix
-// sort).  LSD radix passes run only over the 8-bit windows covering the
-// depth bits that vary inside the tile; equal-depth runs are then put in
-// index order by a short insertion sort (the depth key has float resolution,
-// so short runs are common), or, when some run is longer than kMaxTieRun,
-// the whole tile is sorted again on (depth, index).
+// sort).  LSD radix passes run only over the top `prefix_bits` (16 by
+// default, the autotuner's sort-bit-width knob: 8 to 32) of the depth bits
+// that vary inside the tile, two 8-bit passes at 16; the keys
+// are then in order of that prefix, and each run of equal prefixes is put
+// in (depth, index) order by a short insertion sort.  On the benchmark's
+// views no run is longer than 8 keys (the 16-bit prefix of the depth spread
+// inside a tile is nearly unique); when some run is longer than
+// kMaxTieRun, the whole tile is sorted again on (depth, index).
 #pragma once
 
 #include "gs_kernels.h"
@@ -20,6 +23,24 @@ namespace gs {
 namespace tilesort {
 
 constexpr int kMaxTieRun = 32;
+constexpr int kDefaultPrefixBits = 16;
+
+// The part of the varying depth bits that the radix passes sort: the top
+// `bits` of them (8..32; anything else means the default).  *shift receives
+// the lowest bit of that window; keys with the same key >> *shift form the
+// runs left to the insertion sort.
+__device__ __forceinline__ uint64_t prefix_window(const uint64_t vary_depth, int bits, int* shift)
+{
+    if (bits < 8 || bits > 32) bits = kDefaultPrefixBits;
+    if (!vary_depth) {
+        *shift = 32;
+        return 0;
+    }
+    const int hi = 64 - __clzll((long long)vary_depth);  // one past the highest varying bit
+    const int lo = hi - bits > 32 ? hi - bits : 32;
+    *shift = lo;
+    return vary_depth & (~0ull << lo);
+}
 
 // Views into the CTA's shared memory.
 struct Smem {
@@ -185,36 +206,49 @@ __device__ __forceinline__ bool radix_passes(uint64_t (&k)[IPT], int32_t (&v)[IP
 
 __device__ __forceinline__ uint32_t depth_of(const uint64_t key) { return (uint32_t)(key >> 32); }
 
-// Puts every run of equal depths that starts at one of this thread's items
-// (p = first_p + i * stride) of `keys` (sorted by depth, slot in the low
-// 32 bits) in index order.  Returns true when a run is too long to fix.
+// (depth, index) order of two keys of one tile: a before b?
+__device__ __forceinline__ bool key_before(const uint64_t a, const uint64_t b, const int32_t* __restrict__ slot_gi)
+{
+    const uint32_t da = depth_of(a), db = depth_of(b);
+    if (da != db) return da < db;
+    return __ldg(&slot_gi[(uint32_t)a]) < __ldg(&slot_gi[(uint32_t)b]);
+}
+
+// If position p of `keys` (m keys sorted by the prefix key >> shift, slot in
+// the low 32 bits) starts a run of equal prefixes, puts that run in (depth,
+// index) order.  Returns true when the run is too long to fix this way.
+// Runs are disjoint and every key of a run has the run's prefix, so the
+// threads that fix different runs never disturb one another's tests.
+__device__ __forceinline__ bool fix_run_at(uint64_t* keys, const int m, const int p, const int shift,
+                                           const int32_t* __restrict__ slot_gi)
+{
+    const uint64_t pre = keys[p] >> shift;
+    if ((p > 0 && (keys[p - 1] >> shift) == pre) || p + 1 >= m || (keys[p + 1] >> shift) != pre) return false;
+    int len = 2;
+    while (p + len < m && (keys[p + len] >> shift) == pre && len <= kMaxTieRun) ++len;
+    if (len > kMaxTieRun) return true;
+    for (int x = 1; x < len; ++x) {
+        const uint64_t kx = keys[p + x];
+        int y = x - 1;
+        while (y >= 0 && key_before(kx, keys[p + y], slot_gi)) {
+            keys[p + y + 1] = keys[p + y];
+            --y;
+        }
+        keys[p + y + 1] = kx;
+    }
+    return false;
+}
+
+// fix_run_at for every item of this thread (p = first_p + i * stride).
 template <int IPT>
-__device__ __forceinline__ bool fix_tie_runs(uint64_t* keys, const int m, const int first_p, const int stride,
-                                             const int32_t* __restrict__ slot_gi)
+__device__ __forceinline__ bool fix_prefix_runs(uint64_t* keys, const int m, const int first_p, const int stride,
+                                                const int shift, const int32_t* __restrict__ slot_gi)
 {
     bool too_long = false;
 #pragma unroll
     for (int i = 0; i < IPT; ++i) {
         const int p = first_p + i * stride;
-        if (p >= m) continue;
-        const uint32_t d = depth_of(keys[p]);
-        if ((p > 0 && depth_of(keys[p - 1]) == d) || p + 1 >= m || depth_of(keys[p + 1]) != d) continue;
-        int len = 2;
-        while (p + len < m && depth_of(keys[p + len]) == d && len <= kMaxTieRun) ++len;
-        if (len > kMaxTieRun) {
-            too_long = true;
-            continue;
-        }
-        for (int x = 1; x < len; ++x) {
-            const uint64_t kx = keys[p + x];
-            const int32_t gx = __ldg(&slot_gi[(uint32_t)kx]);
-            int y = x - 1;
-            while (y >= 0 && __ldg(&slot_gi[(uint32_t)keys[p + y]]) > gx) {
-                keys[p + y + 1] = keys[p + y];
-                --y;
-            }
-            keys[p + y + 1] = kx;
-        }
+        if (p < m) too_long |= fix_run_at(keys, m, p, shift, slot_gi);
     }
     return too_long;
 }
@@ -223,7 +257,7 @@ __device__ __forceinline__ bool fix_tie_runs(uint64_t* keys, const int m, const 
 // slot).  Every thread of the CTA must call it; it ends with a barrier.
 template <int NT, int IPT>
 __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const int32_t* __restrict__ slot_gi,
-                          const Smem& sm)
+                          const Smem& sm, const int prefix_bits)
 {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     uint64_t k[IPT];
@@ -242,15 +276,17 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
             v[i] = 0;
         }
     }
-    const uint64_t vary = varying_bits<NT>(o, n, sm.red) & 0xFFFFFFFF00000000ull;
+    int shift;
+    const uint64_t window =
+        prefix_window(varying_bits<NT>(o, n, sm.red) & 0xFFFFFFFF00000000ull, prefix_bits, &shift);
     // the keys carry their slots: no values through these passes
-    if (!radix_passes<NT, IPT, false>(k, v, vary, sm)) {
+    if (!radix_passes<NT, IPT, false>(k, v, window, sm)) {
         // one depth for the whole tile: to shared memory as they are
 #pragma unroll
         for (int i = 0; i < IPT; ++i) sm.k[warp * 32 * IPT + i * 32 + lane] = k[i];
         __syncthreads();
     }
-    const bool too_long = fix_tie_runs<IPT>(sm.k, m, warp * 32 * IPT + lane, 32, slot_gi);
+    const bool too_long = fix_prefix_runs<IPT>(sm.k, m, warp * 32 * IPT + lane, 32, shift, slot_gi);
     if (__syncthreads_or(too_long)) {
         // a long run of equal depths: sort again on (depth, index)
         o = 0;

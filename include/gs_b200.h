@@ -76,6 +76,12 @@ typedef struct gs_render_cfg {
     int32_t views_per_block; /* views the fused projection handles per block (0 = 16) */
     int32_t graph;         /* 1 (default): a frame whose scene, options and views' sizes and outputs repeat
                               is captured once into a CUDA graph and replayed; 0: plain stream launches */
+    int32_t raster_chunk;  /* GS_TERM_TMIN raster: Gaussians each warp culls and stages in shared memory per
+                              step, 32 or 64 (0 = 32) */
+    int32_t raster_persistent; /* GS_TERM_TMIN raster: 1 = persistent CTAs pulling tiles (heavy first) from an
+                              atomic queue; 0 (default) = one CTA per tile */
+    int32_t sort_bits;     /* per-tile depth sort of GS_ORDER_BUCKETS frames: the top varying depth bits sorted by
+                              radix passes, 8..32 (0 = 16); the rest is ordered by insertion within runs */
 } gs_render_cfg;
 
 /* Tile-list ordering of the whole-frame entry points.  Both give the order of
@@ -86,6 +92,9 @@ typedef struct gs_render_cfg {
  * per-tile ranges (the reference's structure, core/gaussian_render.cu:312-677). */
 #define GS_ORDER_BUCKETS 0
 #define GS_ORDER_ONESWEEP 1
+/* Either ordering, as gs_autotune picked it for the batch's bucket (a frame
+ * rendered with it untuned uses GS_ORDER_BUCKETS). */
+#define GS_ORDER_AUTO 2
 
 /* Per-stage device times of one frame, same fields as the reference's
  * RenderStats (core/types.h:26-33), plus the tile-list size. */
@@ -178,11 +187,12 @@ typedef struct gs_tune_result {
     double ms;      /* median device time of one gs_render_batch call */
 } gs_tune_result;
 
-/* Times gs_render_batch of `cams` with the batching knobs swept over their
- * valid values and everything else taken from `base`, and stores the
- * fastest knobs in the context's table under the bucket of (N = the
+/* Times gs_render_batch of `cams` while sweeping the batching knobs, and
+ * stores the fastest in the context's table under the bucket of (N = the
  * scene's size, the largest view's pixel count, num_views, base's
- * termination and ordering); gs_autotune_lookup reads it back.  Swept:
+ * termination and ordering); gs_autotune_lookup reads it back.  The sweep is
+ * a coordinate descent: each knob in turn is timed at all its values with
+ * the others at the best found so far, in this order:
  *   tile shape 16x16 / 16x8 / 8x8   GS_TERM_TMIN only (the reference mode's
  *                                   tile-wide termination is defined on the
  *                                   16x16 tiles it was given; under
@@ -194,18 +204,27 @@ typedef struct gs_tune_result {
  *                                   elsewhere as in the reference, follows
  *                                   the grid);
  *   views_per_block 8 / 16 / 32     batches of more than 8 views;
- *   sort_variant 0..3               GS_ORDER_ONESWEEP only.
- * Each candidate renders 2 untimed frames (the second captures its graph
- * when base->graph is set) and then `iterations` timed ones (>= 1) into
- * context-owned images.  `best` receives base with the winning knobs,
- * `best_ms` its time; `results` (may be NULL) receives up to
+ *   ordering buckets / onesweep     base ordering GS_ORDER_AUTO only;
+ *   sort_variant 0..3               onesweep ordering;
+ *   sort_bits 8 / 16 / 24 / 32      bucket ordering (the per-tile sort's
+ *                                   radix width);
+ *   raster_chunk 32 / 64            GS_TERM_TMIN (Gaussians per
+ *                                   shared-memory batch of the raster);
+ *   raster_persistent 0 / 1         GS_TERM_TMIN.
+ * The sorts are exact, so sort knobs never change an image; raster_chunk
+ * moves where a warp notices that its pixels are done, which changes colours
+ * by less than t_min.  Each candidate renders 2 untimed frames (the second
+ * captures its graph when base->graph is set) and then `iterations` timed
+ * ones (>= 1) into context-owned images.  `best` receives base with the
+ * winning knobs, `best_ms` its time; `results` (may be NULL) receives up to
  * `results_capacity` candidates in the order they were timed and
  * `num_results` (may be NULL) their count.  Synchronous. */
 GS_API int gs_autotune(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, int32_t num_views,
                        const gs_render_cfg* base, int32_t iterations, gs_render_cfg* best, double* best_ms,
                        gs_tune_result* results, int32_t results_capacity, int32_t* num_results, void* stream);
 /* Applies the knobs gs_autotune stored for the bucket of (n, width*height,
- * num_views, cfg->termination, cfg->ordering) to *cfg and sets *found = 1;
+ * num_views, cfg->termination, cfg->ordering) to *cfg (GS_ORDER_AUTO becomes
+ * the tuned ordering) and sets *found = 1;
  * leaves *cfg as it is and sets *found = 0 when that bucket was not tuned.
  * Buckets: N and the pixel count by their power of two (floor log2), the
  * view count by 1, 2-4, 5-8, 9-16, 17-32, 33+. */

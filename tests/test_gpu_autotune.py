@@ -36,17 +36,25 @@ def test_autotune_tmin_sweeps_tile_shapes_and_fills_the_table(gs):
     base = gs.RenderConfig()
     assert gs.autotune_lookup(ctx, n, 640, 480, 4, base) is None
     best, best_ms, results = gs.autotune(ctx, scene, cams, base, iterations=3)
-    # four views: tile shapes only (views per block matters above 8 views)
-    shapes = sorted((r.tile_w, r.tile_h) for r, _ in results)
-    assert shapes == [(8, 8), (16, 8), (16, 16)]
+    # four views: coordinate descent over tile shape, the tile sort's radix
+    # width, the raster's batch and the persistent raster (views per block
+    # matters above 8 views, the onesweep tile shape for onesweep frames)
+    shapes = {(r.tile_w, r.tile_h) for r, _ in results}
+    assert shapes == {(8, 8), (16, 8), (16, 16)}
+    assert {r.sort_bits for r, _ in results} == {8, 16, 24, 32}
+    assert {r.raster_chunk for r, _ in results} == {32, 64}
+    assert {r.raster_persistent for r, _ in results} == {0, 1}
+    assert {r.sort_variant for r, _ in results} == {0}
+    assert len(results) == 3 + 3 + 1 + 1  # a candidate is timed once
     assert all(ms > 0 for _, ms in results)
     assert best_ms == min(ms for _, ms in results)
     assert (best.tile_w, best.tile_h) in shapes
     assert gs.lib.gs_autotune_entries(ctx.h) == 1
     # the bucket: same powers of two of N and pixels, same view-count class
     hit = gs.autotune_lookup(ctx, n + 1000, 700, 500, 3, base)
-    assert hit is not None and (hit.tile_w, hit.tile_h, hit.views_per_block) == \
-        (best.tile_w, best.tile_h, best.views_per_block)
+    assert hit is not None and (hit.tile_w, hit.tile_h, hit.views_per_block, hit.sort_bits, hit.raster_chunk,
+                                hit.raster_persistent) == \
+        (best.tile_w, best.tile_h, best.views_per_block, best.sort_bits, best.raster_chunk, best.raster_persistent)
     assert hit.sh_max_degree == base.sh_max_degree and hit.termination == base.termination
     assert gs.autotune_lookup(ctx, 4 * n, 640, 480, 4, base) is None        # other N bucket
     assert gs.autotune_lookup(ctx, n, 1920, 1080, 4, base) is None          # other resolution bucket
@@ -82,9 +90,11 @@ def test_autotune_reference_mode_keeps_16x16_and_sweeps_views_per_block(gs):
     base = gs.RenderConfig.reference()
     best, best_ms, results = gs.autotune(ctx, scene, cams, base, iterations=2)
     assert {(r.tile_w, r.tile_h) for r, _ in results} == {(16, 16)}
-    assert sorted(r.views_per_block for r, _ in results) == [8, 16, 32]
+    assert {r.views_per_block for r, _ in results} == {8, 16, 32}
+    assert {r.sort_bits for r, _ in results} == {8, 16, 24, 32}
+    assert len(results) == 3 + 3
     assert best.termination == gs.GS_TERM_REFERENCE and best.sh_max_degree == 2
-    # views per block never changes the images
+    # neither views per block nor the sort's radix width changes the images
     want = _batch_images(gs, ctx, scene, cams, base)
     for cfg, _ in results:
         assert np.array_equal(_batch_images(gs, ctx, scene, cams, cfg), want)
@@ -103,8 +113,9 @@ def test_autotune_onesweep_sweeps_sort_variants(gs):
     cams = _cams(gs, 1, 512, 512, 2)
     base = gs.RenderConfig(ordering=1)
     best, _, results = gs.autotune(ctx, scene, cams, base, iterations=1)
-    assert len(results) == 3 * 4
+    assert len(results) == 3 + 3 + 1 + 1
     assert {r.sort_variant for r, _ in results} == {0, 1, 2, 3}
+    assert {r.sort_bits for r, _ in results} == {16}  # the bucket sort's knob does not apply
     assert best.ordering == 1
     hit = gs.autotune_lookup(ctx, n, 512, 512, 1, base)
     assert hit is not None and hit.sort_variant == best.sort_variant
@@ -123,5 +134,31 @@ def test_autotune_rejects_bad_arguments(gs):
     with pytest.raises(gs.GsError):
         gs.autotune(ctx, scene, cams, gs.RenderConfig(tile_w=32, tile_h=32))
     assert gs.lib.gs_autotune_entries(ctx.h) == 0
+    scene.close()
+    ctx.close()
+
+
+def test_autotune_picks_the_ordering_when_asked(gs):
+    """GS_ORDER_AUTO: the tuner times both orderings and the table returns
+    the one it picked; an untuned AUTO frame renders as tile buckets."""
+    ctx = gs.Context(0)
+    n = 60_000
+    sc = gs.scenes.uniform_scene(n, seed=7)
+    scene = gs.Scene(ctx, sc["pos4"], sc["sr4"], gs.scenes.grouped_sh(sc["sh"]), 3, keep_order=True)
+    cams = _cams(gs, 2, 640, 480, 4)
+    auto = gs.RenderConfig(ordering=gs.GS_ORDER_AUTO)
+    assert np.array_equal(_batch_images(gs, ctx, scene, cams, auto), _batch_images(gs, ctx, scene, cams,
+                                                                                    gs.RenderConfig()))
+    best, best_ms, results = gs.autotune(ctx, scene, cams, auto, iterations=1)
+    assert {r.ordering for r, _ in results} == {gs.GS_ORDER_BUCKETS, gs.GS_ORDER_ONESWEEP}
+    assert best.ordering in (gs.GS_ORDER_BUCKETS, gs.GS_ORDER_ONESWEEP)
+    hit = gs.autotune_lookup(ctx, n, 640, 480, 2, auto)
+    assert hit is not None and hit.ordering == best.ordering
+    # a scene in the caller's order: both orderings give the same images
+    want = _batch_images(gs, ctx, scene, cams, gs.RenderConfig())
+    for cfg, _ in results:
+        got = _batch_images(gs, ctx, scene, cams, cfg).reshape(-1, 4)
+        diff = np.abs(got[:, :3].astype(int) - want.reshape(-1, 4)[:, :3].astype(int))
+        assert diff.max() <= 16 and np.percentile(diff, 99.9) <= IMG_TOL
     scene.close()
     ctx.close()
