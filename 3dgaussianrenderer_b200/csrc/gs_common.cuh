@@ -387,9 +387,12 @@ __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0
 
 // The five tests evaluated with the hardware reciprocal, each result kept
 // as the value compared with 1.  Returns 1 (overlap) or 0 (none) when every
-// value lies clearly on one side of 1 (more than 1e-3 away; with the tile's
-// corners within 64 ellipse radii the reciprocals move the values by less
-// than 1e-3, so the IEEE evaluation decides the same), -1 otherwise.
+// value lies clearly on one side of 1 (more than 1e-3 away), -1 otherwise.
+// With every corner within 64 ellipse radii, the reciprocals (a few ulp) and
+// the different rounding of the corners and edges move a value near 1 by
+// well under 1e-4 (each term's error is a few ulp of at most 64^2 ... 2 x 64
+// for the squared lengths near 1 that matter), so where this says clear,
+// the reference's IEEE evaluation decides the same.
 __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
                                                           const float x1, const float y1);
 
@@ -431,38 +434,45 @@ __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const fl
                                                           const float x1, const float y1)
 {
     constexpr float kMargin = 1e-3f;
+    // The tile's image in ellipse coordinates is a parallelogram: corner
+    // (x0, y0) maps to a, the x edge to u, the y edge to v, so the other
+    // corners are a + u, a + u + v, a + v and each edge's squared length is
+    // |u|^2 or |v|^2 -- the same five values as the reference's tests,
+    // rounded differently.
     const float iex = rcp_approx(e.ex), iey = rcp_approx(e.ey);
+    const float dx0 = x0 - e.cx, dy0 = y0 - e.cy;
+    const float ax = (dx0 * e.cs + dy0 * e.sn) * iex, ay = (dy0 * e.cs - dx0 * e.sn) * iey;
+    const float w = x1 - x0, h = y1 - y0;
+    const float ux = (w * e.cs) * iex, uy = -(w * e.sn) * iey;
+    const float vx = (h * e.sn) * iex, vy = (h * e.cs) * iey;
+    // every corner coordinate is at most |a| + |u| + |v| (max norms); far
+    // corners (an edge 64 ellipse radii away) make the rounding matter more
+    // than the margin allows, and a NaN or infinite input lands here too:
+    // let IEEE decide
+    const float far = fmaxf(fabsf(ax), fabsf(ay)) + fmaxf(fabsf(ux), fabsf(uy)) + fmaxf(fabsf(vx), fabsf(vy));
+    if (!(far <= 64.0f)) return -1;
     bool unclear = false;
-    auto test = [&](const float v) {  // v < 1 with its margin
-        if (v < 1.0f - kMargin) return true;
-        if (!(v > 1.0f + kMargin)) unclear = true;  // also NaN
+    auto test = [&](const float val) {  // val < 1 with its margin
+        if (val < 1.0f - kMargin) return true;
+        if (!(val > 1.0f + kMargin)) unclear = true;
         return false;
     };
-    const float rcx = x0 + (x1 - x0) * 0.5f;
-    const float rcy = y0 + (y1 - y0) * 0.5f;
-    float ux, uy;
-    to_ellipse<true>(e, rcx, rcy, ux, uy, iex, iey);
-    if (test(len2(ux, uy))) return 1;
-    float px[4], py[4];
-    to_ellipse<true>(e, x0, y0, px[0], py[0], iex, iey);
-    to_ellipse<true>(e, x1, y0, px[1], py[1], iex, iey);
-    to_ellipse<true>(e, x1, y1, px[2], py[2], iex, iey);
-    to_ellipse<true>(e, x0, y1, px[3], py[3], iex, iey);
-    // far corners (an edge 64 ellipse radii away) make the rounding of the
-    // corners matter more than the margin allows: let IEEE decide
-    const float far = fmaxf(fmaxf(fmaxf(fabsf(px[0]), fabsf(py[0])), fmaxf(fabsf(px[1]), fabsf(py[1]))),
-                            fmaxf(fmaxf(fabsf(px[2]), fabsf(py[2])), fmaxf(fabsf(px[3]), fabsf(py[3]))));
-    if (!(far <= 64.0f)) return -1;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int j = (k + 1) & 3;
-        const float dx = px[j] - px[k], dy = py[j] - py[k];
-        const float l2 = dx * dx + dy * dy;
-        const float t = __saturatef(((-px[k]) * dx + (-py[k]) * dy) * rcp_approx(l2));
-        const float prx = px[k] + t * (px[j] - px[k]);
-        const float pry = py[k] + t * (py[j] - py[k]);
-        if (test(len2(prx, pry))) return 1;
-    }
+    // rect centre in the ellipse
+    if (test(len2(ax + 0.5f * (ux + vx), ay + 0.5f * (uy + vy)))) return 1;
+    // the four edges: the point of segment p + t d (t in [0, 1]) nearest
+    // the origin
+    const float iu = rcp_approx(len2(ux, uy)), iv = rcp_approx(len2(vx, vy));
+    auto edge = [](const float px, const float py, const float dx, const float dy, const float inv) {
+        const float t = __saturatef(-(px * dx + py * dy) * inv);
+        return len2(px + t * dx, py + t * dy);
+    };
+    const float bx = ax + ux, by = ay + uy;  // (x1, y0)
+    const float cx = bx + vx, cy = by + vy;  // (x1, y1)
+    const float qx = ax + vx, qy = ay + vy;  // (x0, y1)
+    if (test(edge(ax, ay, ux, uy, iu))) return 1;
+    if (test(edge(bx, by, vx, vy, iv))) return 1;
+    if (test(edge(cx, cy, -ux, -uy, iu))) return 1;
+    if (test(edge(qx, qy, -vx, -vy, iv))) return 1;
     return unclear ? -1 : 0;
 }
 

@@ -307,6 +307,79 @@ def run_ref_cuda_1024(sc, frames=30):
                         "camera"}
 
 
+def run_sort_vs_cub(gs, ctx, sc, dev, iters=15):
+    """The onesweep sort of gs_stage_sort against the sort the reference
+    calls, CUB's DeviceRadixSort::SortPairs (its sortTileList,
+    core/gaussian_render.cu:591-632, built into oracle/_ref/libgsref.so), on
+    identical (key, value) pairs and key widths, each call timed with CUDA
+    events after the unsorted input is restored: the tile-list keys of the
+    1024x1024 reference-mode frame of the 3M scene (44 bits, the reference's
+    width) and 222M random keys of the 64-view batch's width (51 bits).  The
+    outputs must be identical (both sorts are stable).  Median ms per sort."""
+    import ctypes
+    import torch
+    import oracle
+    if not os.path.exists(oracle.REF_LIB):
+        return None
+    ref = oracle.Ref()
+    out = []
+    # keys of the 1024^2 frame: the stage API's projection and build
+    eye = gs.scenes.orbit_ring(64, RING_RADIUS, seed=1000)[0]
+    cam = gs.look_at(eye, (0, 0, 0), (0, 1, 0), 50.0, 1024, 1024, 0.1, 100.0)
+    n = sc["pos4"].shape[0]
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    xy = torch.zeros((n, 2), dtype=torch.float32, device=dev)
+    z = torch.zeros(n, dtype=torch.float32, device=dev)
+    ell = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    con = torch.zeros((n, 4), dtype=torch.float32, device=dev)
+    gs.stage_project(n, t(sc["pos4"]), t(sc["sr4"]), cam, xy, z, ell, con)
+    cap = 16 * n
+    k = torch.zeros(cap, dtype=torch.int64, device=dev)
+    v = torch.zeros(cap, dtype=torch.int32, device=dev)
+    K = gs.stage_build(ctx, n, xy, z, ell, cam, gs.RenderConfig.reference(), k, v, cap)
+    del xy, z, ell, con
+    cases = [("1024x1024 frame keys, 3M scene", k[:K].clone(), v[:K].clone(), 44)]
+    del k, v
+    m = 222_000_000
+    g = torch.Generator(device=dev)
+    g.manual_seed(5)
+    rk = (torch.randint(0, 1 << 19, (m,), device=dev, generator=g, dtype=torch.int64) << 32) | \
+        torch.randint(0, 1 << 32, (m,), device=dev, generator=g, dtype=torch.int64)
+    rv = torch.arange(m, dtype=torch.int32, device=dev)
+    cases.append(("222M random keys (64-view batch width)", rk, rv, 51))
+    for name, src_k, src_v, bits in cases:
+        cnt = src_k.numel()
+        k0, k1 = torch.empty_like(src_k), torch.empty_like(src_k)
+        v0, v1 = torch.empty_like(src_v), torch.empty_like(src_v)
+        sel = ctypes.c_int(0)
+        cub_ms = ref.lib.gsref_cub_sort_timed(cnt, bits, src_k.data_ptr(), src_v.data_ptr(), k0.data_ptr(),
+                                              k1.data_ptr(), v0.data_ptr(), v1.data_ptr(), iters, ctypes.byref(sel))
+        torch.cuda.synchronize()
+        cub_k = (k1 if sel.value else k0).clone()
+        cub_v = (v1 if sel.value else v0).clone()
+        stream = torch.cuda.current_stream(dev)
+        times = []
+        for _ in range(iters):
+            k0.copy_(src_k)
+            v0.copy_(src_v)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            s_ours = gs.stage_sort(ctx, cnt, bits, k0, v0, k1, v1, stream)
+            e1.record(stream)
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1))
+        ours_k = k1 if s_ours else k0
+        ours_v = v1 if s_ours else v0
+        same = bool(torch.equal(ours_k, cub_k) and torch.equal(ours_v, cub_v))
+        ours_ms = float(np.median(times))
+        out.append({"case": name, "keys": int(cnt), "bits": bits, "cub_ms": float(cub_ms), "ours_ms": ours_ms,
+                    "speedup": float(cub_ms) / ours_ms, "identical_output": same,
+                    "ours_gkeys_s": cnt / ours_ms / 1e6})
+        del k0, k1, v0, v1, cub_k, cub_v
+    return out
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -361,15 +434,23 @@ def run_ours(args, rank, world, local_rank):
     rc = gs.RenderConfig()
     tuned = None
     if not args.no_autotune:
-        # the project's autotuner picks the batching knobs (tile shape, views
-        # per block) for this (N, resolution, views) bucket, outside the
-        # timed region; every rank tunes its own replica
-        best, best_ms, cands = gs.autotune(ctx, scene, cams, rc, iterations=3, stream=stream)
+        # the project's autotuner picks the knobs (tile shape, views per
+        # block, ordering, the tile sort's radix width, the raster's batch of
+        # Gaussians, the persistent raster) for this (N, resolution, views)
+        # bucket by coordinate descent, outside the timed region; every rank
+        # tunes its own replica
+        best, best_ms, cands = gs.autotune(ctx, scene, cams, gs.RenderConfig(ordering=gs.GS_ORDER_AUTO),
+                                           iterations=3, stream=stream)
         rc = best
-        tuned = {"picked": {"tile": f"{best.tile_w}x{best.tile_h}", "views_per_block": best.views_per_block,
-                            "ms": best_ms},
-                 "candidates": [{"tile": f"{c.tile_w}x{c.tile_h}", "views_per_block": c.views_per_block, "ms": m}
-                                for c, m in cands]}
+
+        def knobs(c):
+            return {"tile": f"{c.tile_w}x{c.tile_h}", "views_per_block": c.views_per_block,
+                    "ordering": "onesweep" if c.ordering == gs.GS_ORDER_ONESWEEP else "buckets",
+                    "sort_variant": c.sort_variant, "sort_bits": c.sort_bits, "raster_chunk": c.raster_chunk,
+                    "raster_persistent": c.raster_persistent}
+
+        tuned = {"picked": dict(knobs(best), ms=best_ms), "search": "coordinate descent",
+                 "candidates": [dict(knobs(c), ms=m) for c, m in cands]}
     outs = [torch.empty((c.GetHeight(), c.GetWidth(), 4), dtype=torch.uint8, device=dev) for c in cams]
 
     def step():
@@ -466,6 +547,17 @@ def run_ours(args, rank, world, local_rank):
             clk1024.mark_end()
             ref1024["clocks"] = clk1024.stop()
 
+    sort_vs_cub = None
+    if rank == 0 and not args.no_ref_cuda and not args.no_plain:
+        clk_sort = Clocks(local_rank)
+        clk_sort.mark_start()
+        sort_vs_cub = run_sort_vs_cub(gs, ctx, sc, dev)
+        clk_sort.mark_end()
+        clocks_sort = clk_sort.stop()
+        if sort_vs_cub:
+            sort_vs_cub = {"cases": sort_vs_cub, "clocks": clocks_sort}
+        torch.cuda.empty_cache()
+
     served = None
     if not args.no_serve:
         # release this leg's frame buffers first: the server has its own
@@ -539,6 +631,7 @@ def run_ours(args, rank, world, local_rank):
         "plain_views_per_s": plain_value,
         "batched_over_plain": (value / world / plain_value) if plain_value else None,
         "plain_ref_mode_1024": ref1024,
+        "sort_vs_cub": sort_vs_cub,
         "served": served,
         "roofline": roof,
         "frame_roofline": frame_roof,

@@ -278,10 +278,12 @@ class Ref:
             "gsref_probe_overlap": (ctypes.c_int, [ctypes.c_int, _P, _P, _P]),
             "gsref_probe_aabb": (ctypes.c_int, [ctypes.c_int, _P, _P]),
             "gsref_probe_key": (ctypes.c_int, [ctypes.c_int, _P, _P, _P]),
+            "gsref_cub_sort_timed": (F, [ctypes.c_int, ctypes.c_int, _P, _P, _P, _P, _P, _P, ctypes.c_int,
+                                         ctypes.POINTER(ctypes.c_int)]),
         }
         for name, (res, args) in sig.items():
-            if name.startswith("gsref_probe_") and not hasattr(L, name):
-                continue  # the stage-compat build has no device-helper probes
+            if (name.startswith("gsref_probe_") or name == "gsref_cub_sort_timed") and not hasattr(L, name):
+                continue  # the stage-compat build has neither the probes nor CUB
             fn = getattr(L, name)
             fn.restype = res
             fn.argtypes = args

@@ -232,6 +232,70 @@ int gsref_tile_size()
 }
 
 #ifndef GS_HARNESS_STAGE_COMPAT
+// ---- the reference's sort as a timed kernel --------------------------------
+
+// The sort of sortTileList (core/gaussian_render.cu:591-632): CUB's
+// DeviceRadixSort::SortPairs on a DoubleBuffer, bits [0, endBit) -- the
+// reference fixes endBit at 44, this takes it as an argument so the same
+// library sort can be timed on the key widths of other frames.  Each of the
+// `iters` calls first restores the unsorted input (srcKeys/srcVals ->
+// keys0/vals0, outside the timed region), then times one SortPairs with
+// events on the default stream.  Returns the median call time in ms;
+// *selector = 0 when the last result is in keys0/vals0, 1 in keys1/vals1.
+float gsref_cub_sort_timed(int n,
+                           int endBit,
+                           const void* srcKeys,
+                           const void* srcVals,
+                           void* keys0,
+                           void* keys1,
+                           void* vals0,
+                           void* vals1,
+                           int iters,
+                           int* selector)
+{
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float times[256];
+    iters = iters < 1 ? 1 : (iters > 256 ? 256 : iters);
+    for (int it = 0; it < iters; ++it)
+    {
+        cudaMemcpyAsync(keys0, srcKeys, sizeof(uint64_t) * (size_t) n, cudaMemcpyDeviceToDevice);
+        cudaMemcpyAsync(vals0, srcVals, sizeof(int32_t) * (size_t) n, cudaMemcpyDeviceToDevice);
+        cub::DoubleBuffer<uint64_t> k((uint64_t*) keys0, (uint64_t*) keys1);
+        cub::DoubleBuffer<int32_t> v((int32_t*) vals0, (int32_t*) vals1);
+        size_t need = 0;
+        cub::DeviceRadixSort::SortPairs((void*) nullptr, need, k, v, n, 0, endBit);
+        if (need > g_SortTempBytes)
+        {
+            if (g_SortTemp)
+            {
+                cudaFree(g_SortTemp);
+            }
+            cudaMalloc(&g_SortTemp, need);
+            g_SortTempBytes = need;
+        }
+        cudaEventRecord(e0);
+        cub::DeviceRadixSort::SortPairs(g_SortTemp, g_SortTempBytes, k, v, n, 0, endBit);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        cudaEventElapsedTime(&times[it], e0, e1);
+        *selector = (k.Current() == (uint64_t*) keys0) ? 0 : 1;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    for (int i = 1; i < iters; ++i)
+    {
+        for (int j = i; j > 0 && times[j] < times[j - 1]; --j)
+        {
+            const float t = times[j];
+            times[j] = times[j - 1];
+            times[j - 1] = t;
+        }
+    }
+    return times[iters / 2];
+}
+
 // ---- probes of the reference's device helpers ------------------------------
 
 // ell: n x 6 floats (centre.x, centre.y, cos, sin, extent.x, extent.y)

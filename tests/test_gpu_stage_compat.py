@@ -83,6 +83,10 @@ def test_saturated_tile_list_is_truncated_like_the_reference(compat, gs):
             (("xy", (n, 2)), ("z", (n,)), ("conic", (n, 4)), ("ell", (n, 4)))}
     img = torch.zeros((1024, 1024, 4), dtype=torch.uint8, device=dev)
     ranges = torch.zeros(2 * 4096, dtype=torch.int32, device=dev)
+    # device copies held for the whole loop (a temporary's memory is freed
+    # as soon as only its address is kept)
+    pos, sr = t(sc["pos4"]), t(sc["sr4"])
+    cam56 = oracle.Ref.camera56(cam)
     K = int(d["ref_K"])
     for cap in (K // 3, K):
         keys = [torch.zeros(cap, dtype=torch.int64, device=dev) for _ in range(2)]
@@ -91,7 +95,7 @@ def test_saturated_tile_list_is_truncated_like_the_reference(compat, gs):
         fms = ctypes.c_float(0)
         sel = ctypes.c_int(0)
         size = compat.lib.gsref_render_frame(
-            oracle.Ref.camera56(cam).ctypes.data, t(sc["pos4"]).data_ptr(), t(sc["sr4"]).data_ptr(),
+            cam56.ctypes.data, pos.data_ptr(), sr.data_ptr(),
             color.data_ptr(), deg, 3 * (deg + 1) ** 2, sh.data_ptr(), bufs["xy"].data_ptr(), bufs["z"].data_ptr(),
             bufs["conic"].data_ptr(), bufs["ell"].data_ptr(), n, img.data_ptr(), ranges.data_ptr(),
             keys[0].data_ptr(), keys[1].data_ptr(), vals[0].data_ptr(), vals[1].data_ptr(), cap, 148 * 8, ms,
