@@ -396,28 +396,20 @@ __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0
 __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
                                                           const float x1, const float y1);
 
-// ellipseRectOverlap (gaussian_render.cu:250-272): the centre-in-rectangle
-// test, then the other four of the reference's five tests in IEEE
-// arithmetic wherever the approximate evaluation is not clear of the
-// threshold.  Bit-exact with the reference on every input.
-__device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x0, const float y0, const float x1,
-                                                     const float y1)
+// The reference's four tests after its centre-in-rectangle test, in IEEE
+// arithmetic (gaussian_render.cu:250-272).  Not inlined: it runs only for
+// the rare values the cheap evaluation cannot decide, and keeping its
+// divisions out of the callers' loops keeps their registers from spilling.
+static __device__ __noinline__ bool ellipse_rect_overlap_ieee(const Ell e, const float x0, const float y0, const float x1,
+                                                       const float y1)
 {
-    bool ov = e.cx > x0 && e.cx < x1 && e.cy > y0 && e.cy < y1;
-    // The reference ORs all five tests, so a centre strictly inside the tile
-    // decides the result; skipping the rest changes nothing.
-    if (ov) return true;
-    // the approximate evaluation decides whenever it is clear of the
-    // threshold; only near-boundary cases run the IEEE divisions
-    const int clear = ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
-    if (clear >= 0) return clear != 0;
     const float iex = 0.0f, iey = 0.0f;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
     const float rcy = y0 + (y1 - y0) * 0.5f;
     float ux, uy;
     to_ellipse<false>(e, rcx, rcy, ux, uy, iex, iey);
-    ov |= len2(ux, uy) < 1.0f;
+    bool ov = len2(ux, uy) < 1.0f;
     float p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y;
     to_ellipse<false>(e, x0, y0, p0x, p0y, iex, iey);
     to_ellipse<false>(e, x1, y0, p1x, p1y, iex, iey);
@@ -428,6 +420,21 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
     ov |= hits_unit_circle(p2x, p2y, p3x, p3y);
     ov |= hits_unit_circle(p3x, p3y, p0x, p0y);
     return ov;
+}
+
+// ellipseRectOverlap (gaussian_render.cu:250-272): the centre-in-rectangle
+// test, then the other four of the reference's five tests, decided by a
+// cheap evaluation wherever it is clear of the threshold and in IEEE
+// arithmetic otherwise.  Bit-exact with the reference on every input.
+__device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x0, const float y0, const float x1,
+                                                     const float y1)
+{
+    // The reference ORs all five tests, so a centre strictly inside the tile
+    // decides the result; skipping the rest changes nothing.
+    if (e.cx > x0 && e.cx < x1 && e.cy > y0 && e.cy < y1) return true;
+    const int clear = ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
+    if (clear >= 0) return clear != 0;
+    return ellipse_rect_overlap_ieee(e, x0, y0, x1, y1);
 }
 
 __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
@@ -552,23 +559,50 @@ __device__ __forceinline__ void divmod_small(const int c, const int d, int& q, i
     r = rr;
 }
 
-// Candidate c of a tile rectangle, row-major (gaussian_render.cu:466-483).
-// Returns true on overlap and the view-local tile index.
-__device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const int c, const ViewParams& v, int& tile)
+// Clip-space rectangle of tile (gx, gy) (gaussian_render.cu:471-473).
+__device__ __forceinline__ void tile_clip_rect(const ViewParams& v, const int gx, const int gy, float& x0, float& y0,
+                                               float& x1, float& y1)
+{
+    x0 = (float)gx * v.tclip_x - 1.0f;
+    y0 = (float)gy * v.tclip_y - 1.0f;
+    x1 = x0 + v.tclip_x;
+    y1 = y0 + v.tclip_y;
+}
+
+// Candidate c of a tile rectangle, row-major (gaussian_render.cu:466-483),
+// tested without the IEEE evaluation: 1 = overlap, 0 = none, -1 = too close
+// to call (candidate_hit_ieee decides).  Sets the view-local tile index
+// whenever the candidate lies on screen.  Off-screen candidates only arise
+// from the inverted rectangles of NaN axes; their centre test cannot pass
+// for a visible splat, so they never overlap.
+__device__ __forceinline__ int candidate_state(const Ell& e, const int4 r, const int c, const ViewParams& v, int& tile)
 {
     int lx, ly;
     divmod_small(c, r.z, ly, lx);
     const int gx = r.x + lx, gy = r.y + ly;
-    const float tx0 = (float)gx * v.tclip_x - 1.0f;
-    const float ty0 = (float)gy * v.tclip_y - 1.0f;
-    const float tx1 = tx0 + v.tclip_x;
-    const float ty1 = ty0 + v.tclip_y;
-    if (!ellipse_rect_overlap(e, tx0, ty0, tx1, ty1)) return false;
-    // Off-screen candidates only arise from the inverted rectangles of NaN
-    // axes; their centre test cannot pass for a visible splat.
-    if (gx < 0 || gx >= v.tiles_x || gy < 0 || gy >= v.tiles_y) return false;
+    if (gx < 0 || gx >= v.tiles_x || gy < 0 || gy >= v.tiles_y) return 0;
     tile = gy * v.tiles_x + gx;
-    return true;
+    float x0, y0, x1, y1;
+    tile_clip_rect(v, gx, gy, x0, y0, x1, y1);
+    if (e.cx > x0 && e.cx < x1 && e.cy > y0 && e.cy < y1) return 1;  // centre in the tile decides
+    return ellipse_rect_overlap_clear(e, x0, y0, x1, y1);
+}
+
+// The IEEE decision of a candidate that candidate_state could not call.
+__device__ __forceinline__ bool candidate_hit_ieee(const Ell& e, const int tile, const ViewParams& v)
+{
+    float x0, y0, x1, y1;
+    tile_clip_rect(v, tile % v.tiles_x, tile / v.tiles_x, x0, y0, x1, y1);
+    return ellipse_rect_overlap_ieee(e, x0, y0, x1, y1);
+}
+
+// Candidate c of a tile rectangle: true on overlap (exactly the reference's
+// test), with the view-local tile index.
+__device__ __forceinline__ bool candidate_hit(const Ell& e, const int4 r, const int c, const ViewParams& v, int& tile)
+{
+    const int st = candidate_state(e, r, c, v, tile);
+    if (st >= 0) return st != 0;
+    return candidate_hit_ieee(e, tile, v);
 }
 
 // getKey (gaussian_render.cu:306-310): tile << 32 | quantised depth.

@@ -99,6 +99,23 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
 // and when a frame has few tiles, many atomics on one address serialise.
 // With many tiles the atomics spread out and the grouping costs more than
 // it saves.
+//
+// The overlap test is the reference's, in two phases: the walk decides every
+// candidate the cheap evaluation can call, and only if some candidate of the
+// warp was too close to call does a second walk settle those in IEEE
+// arithmetic.  Keeping the IEEE code out of the first walk keeps it free of
+// register spills.
+__device__ __forceinline__ void add_hits(const unsigned bal, const WarpCands& w, const int base, const int cand,
+                                         int& hits, uint32_t& mask)
+{
+    const unsigned bits = bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32));
+    if (bits) {
+        hits += __popc(bits);
+        // lane l of this chunk is candidate base + l - excl of its owner
+        if (cand <= 32) mask |= (w.excl >= base) ? (bits >> (w.excl - base)) : (bits << (base - w.excl));
+    }
+}
+
 __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
                                                uint32_t& mask, uint32_t* tile_count = nullptr,
                                                const bool aggregate = false)
@@ -107,27 +124,33 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
     const WarpCands w = warp_scan_cands(cand);
     int hits = 0;
     mask = 0u;
-    for (int base = 0; base < w.total; base += 32) {
-        const int c = base + lane;
-        const int o = owner_of(w.incl, c);
-        Ell oe;
+    bool undecided = false;
+    auto owner_ell = [&](const int o, Ell& oe, int4& orr) {
         oe.cx = __shfl_sync(kFull, e.cx, o);
         oe.cy = __shfl_sync(kFull, e.cy, o);
         oe.cs = __shfl_sync(kFull, e.cs, o);
         oe.sn = __shfl_sync(kFull, e.sn, o);
         oe.ex = __shfl_sync(kFull, e.ex, o);
         oe.ey = __shfl_sync(kFull, e.ey, o);
-        int4 orr;
         orr.x = __shfl_sync(kFull, r.x, o);
         orr.y = __shfl_sync(kFull, r.y, o);
         orr.z = __shfl_sync(kFull, r.z, o);
         orr.w = __shfl_sync(kFull, r.w, o);
+    };
+    for (int base = 0; base < w.total; base += 32) {
+        const int c = base + lane;
+        const int o = owner_of(w.incl, c);
+        Ell oe;
+        int4 orr;
+        owner_ell(o, oe, orr);
         const int oexcl = __shfl_sync(kFull, w.excl, o);
-        bool hit = false;
+        int st = 0;
         int tile = 0;
-        if (c < w.total) hit = candidate_hit(oe, orr, c - oexcl, v, tile);
+        if (c < w.total) st = candidate_state(oe, orr, c - oexcl, v, tile);
+        undecided |= st < 0;
+        const bool hit = st > 0;
         const unsigned bal = __ballot_sync(kFull, hit);
-if (tile_count && hit) {
+        if (tile_count && hit) {
             if (aggregate) {
                 const unsigned grp = __match_any_sync(bal, tile);
                 if (lane == __ffs(grp) - 1) atomicAdd(&tile_count[v.tile_offset + tile], (unsigned)__popc(grp));
@@ -135,11 +158,24 @@ if (tile_count && hit) {
                 atomicAdd(&tile_count[v.tile_offset + tile], 1u);
             }
         }
-        const unsigned bits = bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32));
-        if (bits) {
-            hits += __popc(bits);
-            // lane l of this chunk is candidate base + l - excl of its owner
-            if (cand <= 32) mask |= (w.excl >= base) ? (bits >> (w.excl - base)) : (bits << (base - w.excl));
+        add_hits(bal, w, base, cand, hits, mask);
+    }
+    if (__any_sync(kFull, undecided)) {
+        // rare: the candidates too close to call, in IEEE arithmetic
+        for (int base = 0; base < w.total; base += 32) {
+            const int c = base + lane;
+            const int o = owner_of(w.incl, c);
+            Ell oe;
+            int4 orr;
+            owner_ell(o, oe, orr);
+            const int oexcl = __shfl_sync(kFull, w.excl, o);
+            int tile = 0;
+            bool hit = false;
+            if (c < w.total && candidate_state(oe, orr, c - oexcl, v, tile) < 0) hit = candidate_hit_ieee(oe, tile, v);
+            const unsigned bal = __ballot_sync(kFull, hit);
+            if (!bal) continue;
+            if (tile_count && hit) atomicAdd(&tile_count[v.tile_offset + tile], 1u);
+            add_hits(bal, w, base, cand, hits, mask);
         }
     }
     return hits;
