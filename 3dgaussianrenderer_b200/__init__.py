@@ -163,6 +163,8 @@ _sig("gs_stage_build", _I, _P, _I64, _P, _P, _P, ctypes.POINTER(gs_camera), ctyp
      _I64, ctypes.POINTER(_I64), _P)
 _sig("gs_stage_sort", _I, _P, _I64, _I32, _P, _P, _P, _P, ctypes.POINTER(_I32), _P)
 _sig("gs_stage_ranges", _I, _I64, _P, _I64, _P, _P)
+_sig("gs_probe_sort_timed", _I, _P, _I64, _I32, _P, _P, _P, _P, _P, _P, _I32, ctypes.POINTER(_I32),
+     ctypes.POINTER(ctypes.c_double))
 _sig("gs_stage_raster", _I, ctypes.POINTER(gs_camera), ctypes.POINTER(gs_render_cfg), _P, _P, _P, _P, _P, _P, _P)
 _sig("gs_probe_frame", _I, _P, _P, ctypes.POINTER(gs_camera), _I32, ctypes.POINTER(gs_render_cfg), ctypes.POINTER(_P),
      ctypes.POINTER(gs_frame_probe), ctypes.POINTER(gs_stats), _P)
@@ -528,6 +530,19 @@ def stage_sort(ctx: Context, num_keys, bits, d_keys, d_values, d_keys_alt, d_val
     check(lib.gs_stage_sort(ctx.h, num_keys, bits, _ptr(d_keys), _ptr(d_values), _ptr(d_keys_alt),
                             _ptr(d_values_alt), ctypes.byref(sel), _stream_ptr(stream)), "gs_stage_sort")
     return int(sel.value)
+
+
+def probe_sort_timed(ctx: Context, num_keys, bits, src_keys, src_values, d_keys, d_values, d_keys_alt,
+                     d_values_alt, iterations: int = 15):
+    """gs_probe_sort_timed: the onesweep sort alone between CUDA events, the
+    unsorted input restored before each of `iterations` runs.  Returns
+    (selector, median ms)."""
+    sel = _I32(0)
+    ms = ctypes.c_double()
+    check(lib.gs_probe_sort_timed(ctx.h, num_keys, bits, _ptr(src_keys), _ptr(src_values), _ptr(d_keys),
+                                  _ptr(d_values), _ptr(d_keys_alt), _ptr(d_values_alt), iterations,
+                                  ctypes.byref(sel), ctypes.byref(ms)), "gs_probe_sort_timed")
+    return int(sel.value), ms.value
 
 
 def stage_ranges(num_keys, d_keys, tiles, d_ranges, stream=None):

@@ -951,8 +951,10 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         stats->num_keys = ctx->h_counters->total;
         stats->num_tiles = p.tiles_total;
         // frame kernel, bucket emit, big-tile sort; tile scan, tile order,
-        // raster (sorts the other tiles)
-        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 3;
+        // raster (sorts the other tiles; one launch per view group when the
+        // images stream to host memory group by group)
+        const bool grouped = p.host_copy && p.host_copy->groups > 1 && cfg.termination == GS_TERM_TMIN;
+        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 2 + (grouped ? p.host_copy->groups : 1);
         stats->graph_replay = replayed ? 1 : 0;
         stats->attempts = attempts;
     }
@@ -1674,6 +1676,53 @@ int gs_stage_sort(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, uint64_t* d_k
     GS_CUDA(cudaMemcpyAsync(&ctx->h_counters->err, &dc->err, sizeof(int), cudaMemcpyDeviceToHost, st));
     GS_CUDA(cudaStreamSynchronize(st));
     if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "sort look-back timed out");
+    *out_selector = passes % 2;
+    return GS_OK;
+}
+
+int gs_probe_sort_timed(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, const uint64_t* d_src_keys,
+                        const int32_t* d_src_values, uint64_t* d_keys, int32_t* d_values, uint64_t* d_keys_alt,
+                        int32_t* d_values_alt, int32_t iterations, int32_t* out_selector, double* out_median_ms)
+{
+    if (!ctx || !out_selector || !out_median_ms || num_keys <= 0 || key_bits < 1 || key_bits > 64 || iterations < 1)
+        return fail(GS_ERR_INVALID, "bad argument");
+    if (num_keys >= (1ll << 31)) return fail(GS_ERR_INVALID, "too many keys");
+    if (!d_src_keys || !d_src_values || !d_keys || !d_values || !d_keys_alt || !d_values_alt)
+        return fail(GS_ERR_INVALID, "null buffer");
+    std::lock_guard<std::mutex> lock(ctx->mu);
+    GS_CUDA(cudaSetDevice(ctx->device));
+    const cudaStream_t st = nullptr;
+    int rc = ensure_sort_scratch(ctx, num_keys);
+    if (rc) return rc;
+    Counters* dc = ctx->counters.as<Counters>();
+    std::vector<double> ms;
+    int passes = 0;
+    for (int it = 0; it < iterations; ++it) {
+        // restore the unsorted input and clear the error flag, outside the
+        // timed region
+        GS_CUDA(cudaMemcpyAsync(d_keys, d_src_keys, sizeof(uint64_t) * (size_t)num_keys, cudaMemcpyDeviceToDevice, st));
+        GS_CUDA(cudaMemcpyAsync(d_values, d_src_values, sizeof(int32_t) * (size_t)num_keys, cudaMemcpyDeviceToDevice,
+                                st));
+        GS_CUDA(cudaMemsetAsync(dc, 0, sizeof(Counters), st));
+        SortScratch ss;
+        ss.hist = ctx->sort_hist.as<uint32_t>();
+        ss.status = ctx->sort_status.as<uint64_t>();
+        ss.counters = dc->sort_tiles;
+        ss.err = &dc->err;
+        ss.max_tiles = (int64_t)(ctx->sort_status.bytes / (8 * kRadix));
+        const uint32_t ep = take_epochs(ctx->epoch_sort, (uint32_t)sort_passes(key_bits), ctx->sort_status, st);
+        GS_CUDA(cudaEventRecord(ctx->ev[6], st));
+        passes = launch_sort(d_keys, d_values, d_keys_alt, d_values_alt, num_keys, nullptr, key_bits, ss, ep,
+                             ctx->num_sms, st);
+        GS_CUDA(cudaGetLastError());
+        GS_CUDA(cudaEventRecord(ctx->ev[7], st));
+        GS_CUDA(cudaMemcpyAsync(&ctx->h_counters->err, &dc->err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GS_CUDA(cudaStreamSynchronize(st));
+        if (ctx->h_counters->err) return fail(GS_ERR_DEVICE_TIMEOUT, "sort look-back timed out");
+        ms.push_back(ms_between(ctx->ev[6], ctx->ev[7]));
+    }
+    std::sort(ms.begin(), ms.end());
+    *out_median_ms = ms[ms.size() / 2];
     *out_selector = passes % 2;
     return GS_OK;
 }

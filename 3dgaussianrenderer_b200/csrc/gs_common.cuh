@@ -387,12 +387,19 @@ __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0
 
 // The five tests evaluated with the hardware reciprocal, each result kept
 // as the value compared with 1.  Returns 1 (overlap) or 0 (none) when every
-// value lies clearly on one side of 1 (more than 1e-3 away), -1 otherwise.
-// With every corner within 64 ellipse radii, the reciprocals (a few ulp) and
-// the different rounding of the corners and edges move a value near 1 by
-// well under 1e-4 (each term's error is a few ulp of at most 64^2 ... 2 x 64
-// for the squared lengths near 1 that matter), so where this says clear,
-// the reference's IEEE evaluation decides the same.
+// value lies clearly on one side of 1, -1 otherwise.  "Clearly" is a margin
+// from an error bound.  Both evaluations start from the same corners, centre,
+// axis and extents.  Let R be D / min(ex, ey), where D bounds the image-space
+// offsets |dx| + |dy| of the corners from the centre.  Every ellipse
+// coordinate either side computes is then within about 25 u R of the exact
+// one (u = 2^-24): the offset, product, sum and division roundings, and the
+// reciprocal's ulp.  A distance to a segment moves by at most its endpoints'
+// displacement, and its own evaluation adds a few u R more, so each compared
+// value differs between the two evaluations by under about 100 u R plus a
+// few u.  An emulation of both in single precision (2M candidates up to
+// R = 1500, contracted and uncontracted products, reciprocals 1 ulp off either
+// way) found at most 2.1 u R + 340 u.  The margin is 256 u R + 2^-15, so where
+// this says clear, the reference's IEEE evaluation decides the same.
 __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
                                                           const float x1, const float y1);
 
@@ -440,28 +447,31 @@ __device__ __forceinline__ bool ellipse_rect_overlap(const Ell& e, const float x
 __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const float x0, const float y0,
                                                           const float x1, const float y1)
 {
-    constexpr float kMargin = 1e-3f;
     // The tile's image in ellipse coordinates is a parallelogram: corner
     // (x0, y0) maps to a, the x edge to u, the y edge to v, so the other
     // corners are a + u, a + u + v, a + v and each edge's squared length is
     // |u|^2 or |v|^2 -- the same five values as the reference's tests,
     // rounded differently.
+    // A zero extent -- every splat whose covariance sits at the trace bump
+    // (mid^2 - det under the eps floor makes lambda1 = 0): the reference's
+    // divisions give +-inf or NaN in that axis, no value compares below 1,
+    // and only the centre-in-rectangle test (the caller's) can pass.
+    if (e.ex == 0.0f || e.ey == 0.0f) return 0;
     const float iex = rcp_approx(e.ex), iey = rcp_approx(e.ey);
     const float dx0 = x0 - e.cx, dy0 = y0 - e.cy;
     const float ax = (dx0 * e.cs + dy0 * e.sn) * iex, ay = (dy0 * e.cs - dx0 * e.sn) * iey;
     const float w = x1 - x0, h = y1 - y0;
     const float ux = (w * e.cs) * iex, uy = -(w * e.sn) * iey;
     const float vx = (h * e.sn) * iex, vy = (h * e.cs) * iey;
-    // every corner coordinate is at most |a| + |u| + |v| (max norms); far
-    // corners (an edge 64 ellipse radii away) make the rounding matter more
-    // than the margin allows, and a NaN or infinite input lands here too:
-    // let IEEE decide
-    const float far = fmaxf(fabsf(ax), fabsf(ay)) + fmaxf(fabsf(ux), fabsf(uy)) + fmaxf(fabsf(vx), fabsf(vy));
-    if (!(far <= 64.0f)) return -1;
+    // margin from R (above); a NaN or infinite input or a corner thousands
+    // of radii away lands here too: let IEEE decide
+    const float R = (fabsf(dx0) + fabsf(dy0) + w + h) * fmaxf(fabsf(iex), fabsf(iey));
+    const float margin = fmaf(R, 256.0f / 16777216.0f, 1.0f / 32768.0f);
+    if (!(margin <= 0.125f)) return -1;
     bool unclear = false;
     auto test = [&](const float val) {  // val < 1 with its margin
-        if (val < 1.0f - kMargin) return true;
-        if (!(val > 1.0f + kMargin)) unclear = true;
+        if (val < 1.0f - margin) return true;
+        if (!(val > 1.0f + margin)) unclear = true;
         return false;
     };
     // rect centre in the ellipse

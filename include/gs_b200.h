@@ -421,6 +421,18 @@ GS_API int gs_probe_tile_lists(gs_ctx* ctx, int32_t* h_ranges, int64_t ranges_ca
                                int32_t* h_order, int64_t keys_capacity, int32_t* h_slot_index, int64_t slots_capacity,
                                int64_t out_sizes[3], int32_t* out_fused_cap);
 
+/* No counterpart in the reference.  Times gs_stage_sort's onesweep sort
+ * alone, for a like-for-like comparison with a library sort timed around
+ * its own call: `iterations` times, the unsorted (d_src_keys, d_src_values)
+ * are copied into (d_keys, d_values) and the sort runs between two CUDA
+ * events on the legacy default stream, with nothing else in the timed
+ * region.  *out_median_ms = the median, *out_selector as gs_stage_sort's.
+ * Synchronous. */
+GS_API int gs_probe_sort_timed(gs_ctx* ctx, int64_t num_keys, int32_t key_bits, const uint64_t* d_src_keys,
+                               const int32_t* d_src_values, uint64_t* d_keys, int32_t* d_values, uint64_t* d_keys_alt,
+                               int32_t* d_values_alt, int32_t iterations, int32_t* out_selector,
+                               double* out_median_ms);
+
 /* ---- failure-path test hooks -------------------------------------------- */
 /* No counterpart in the reference, which exits the process on any CUDA
  * error (core/cuda_error_check.h:2-11).  These let tests exercise the error
