@@ -352,9 +352,12 @@ void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st)
 //
 // Tiles up to the fused capacity are sorted by the raster CTA itself
 // (gs_tilesort.cuh).  The larger ones, listed by the tile scan, are sorted
-// here beforehand -- in shared memory up to kTileSortSmemKeys keys, else by
-// stable LSD passes through global memory -- and their order is written to
-// `vals` for the rasteriser to read.
+// here beforehand -- up to kTileSortSmemKeys keys by one counting pass in
+// shared memory and ranks inside its runs (tilesort::count_sort_tile; the
+// radix form of the raster CTA when a run is too long), else by stable LSD
+// passes through global memory -- and their order is written to `vals` for
+// the rasteriser to read.  On the 64-view batch (57k such tiles, 92M keys)
+// the counting form takes 1.98 ms against 2.33 ms for the radix form.
 
 namespace {
 
@@ -473,11 +476,27 @@ __device__ void sort_big_smem(const TileSortArgs& a, const int64_t start, const 
     for (int p = threadIdx.x; p < m; p += kBigThreads) a.vals[start + p] = (int32_t)(uint32_t)sm.k[p];
 }
 
+// The counting form (one placement pass, ranks inside the runs), the
+// histogram in the values' part of shared memory; a tile with a long run of
+// equal prefixes takes the radix form.
+__device__ void sort_big_count(const TileSortArgs& a, const int64_t start, const int m, const Smem& sm)
+{
+    uint32_t* hist = reinterpret_cast<uint32_t*>(sm.v);
+    const bool long_run =
+        m <= kBigThreads * 8
+            ? tilesort::count_sort_tile<kBigThreads, 8>(a.keys + start, m, a.slot_gi, sm, hist, a.vals + start)
+            : tilesort::count_sort_tile<kBigThreads, 0>(a.keys + start, m, a.slot_gi, sm, hist, a.vals + start);
+    if (!long_run) return;
+    if (m <= 2048)
+        sort_big_smem<8>(a, start, m, sm);
+    else
+        sort_big_smem<16>(a, start, m, sm);
+}
+
 }  // namespace
 
 // Persistent CTAs over the big-tile list.
-// 4 blocks per SM (64 registers, some spilled) measured faster than 2
-// blocks without spills: the passes wait on shared memory and barriers
+// 4 blocks per SM (64 registers; the spills are in the radix fallback)
 constexpr int kBigBlocksPerSm = 4;
 __global__ void __launch_bounds__(kBigThreads, kBigBlocksPerSm) tile_sort_big_kernel(TileSortArgs a)
 {
@@ -502,10 +521,8 @@ __global__ void __launch_bounds__(kBigThreads, kBigBlocksPerSm) tile_sort_big_ke
         const int64_t t = a.big_list[j];
         const int64_t start = __ldg(&a.ranges[2 * t]);
         const int m = __ldg(&a.ranges[2 * t + 1]) - (int)start;
-        if (m <= 2048)
-            sort_big_smem<8>(a, start, m, sm);
-        else if (m <= kTileSortSmemKeys)
-            sort_big_smem<16>(a, start, m, sm);
+        if (m <= kTileSortSmemKeys)
+            sort_big_count(a, start, m, sm);
         else
             sort_tile_global(a, start, m, sm);
         __syncthreads();  // shared memory is reused by the next tile

@@ -1,7 +1,8 @@
 // Block-level sort of one tile's bucket in shared memory, for CTAs of NT
-// threads (32..256).  Used by the rasterisers (tiles of up to
+// threads (32..256).  sort_tile is used by the rasterisers (tiles of up to
 // NT * kFusedIpt keys are sorted by the raster CTA itself, right before
-// blending) and by the stand-alone sort of the larger tiles.
+// blending); the stand-alone sort of the larger tiles uses count_sort_tile
+// (below) and falls back on sort_tile.
 //
 // Keys are (depth << 32 | slot).  The order produced is depth first and,
 // among equal depths, the (view * n + i) index of the slot -- the order of
@@ -310,6 +311,130 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
         }
         __syncthreads();
     }
+}
+
+// Counting-sort form of sort_tile for the stand-alone sort of the larger
+// tiles (m <= kTileSortSmemKeys keys, NT threads), writing the tile's slots
+// in (depth, index) order to `out`.  One pass places every key in shared
+// memory by the top kCountBits varying depth bits: a histogram of 16-bit
+// counters packed two to a word (`hist`, 2^(kCountBits - 1) words; counts
+// and offsets stay below 2^16), its exclusive scan, then each key takes the
+// next position of its bin with a shared-memory atomic, so inside a bin the
+// keys land in no particular order.  After the placement the histogram
+// holds every bin's end, and each key's bin is the run [end(d - 1), end(d))
+// of the keys with its prefix: the key's rank among them in (depth, index)
+// order, counted by the key's own thread, is its offset in the run.  That
+// is the whole order (keys of different bins are ordered by the bin), so
+// the pass need not be stable, and a run of L keys costs L comparisons per
+// key, in parallel.  On the benchmark's views no run is longer than 25 keys.
+// IPT > 0: m <= NT * IPT, each thread holds its IPT keys in registers
+// across the passes; IPT = 0: every pass reads the keys from global memory
+// (the larger tiles).
+// Returns true -- nothing written -- when some run is longer than
+// kMaxRankRun; the caller then sorts the tile another way.  Every thread of
+// the CTA must call it; it ends with a barrier.
+constexpr int kCountBits = 13;
+constexpr int kMaxRankRun = 64;
+
+template <int NT, int IPT>
+__device__ bool count_sort_tile(const uint64_t* __restrict__ keys, const int m, const int32_t* __restrict__ slot_gi,
+                                const Smem& sm, uint32_t* hist, int32_t* __restrict__ out)
+{
+    constexpr int NW = NT / 32;
+    constexpr int kBins = 1 << kCountBits;
+    constexpr int kWords = kBins / 2;
+    constexpr int WPW = kWords / NW;  // histogram words scanned by each warp
+    static_assert(WPW % 32 == 0, "histogram words per warp");
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    uint64_t o = 0, n = ~0ull;
+    uint64_t kr[IPT > 0 ? IPT : 1];
+    if constexpr (IPT > 0) {
+#pragma unroll
+        for (int i = 0; i < IPT; ++i) {
+            const int p = i * NT + threadIdx.x;
+            kr[i] = p < m ? keys[p] : 0ull;
+            if (p < m) {
+                o |= kr[i];
+                n &= kr[i];
+            }
+        }
+    } else {
+        for (int p = threadIdx.x; p < m; p += NT) {
+            const uint64_t k = keys[p];
+            o |= k;
+            n &= k;
+        }
+    }
+    for (int w = threadIdx.x; w < kWords; w += NT) hist[w] = 0u;
+    int shift;
+    prefix_window(varying_bits<NT>(o, n, sm.red) & 0xFFFFFFFF00000000ull, kCountBits, &shift);
+    // (varying_bits ends with a barrier: the cleared histogram is visible)
+    auto count = [&](const uint64_t k) {
+        const uint32_t d = (uint32_t)(k >> shift) & (kBins - 1);
+        atomicAdd(&hist[d >> 1], 1u << ((d & 1u) << 4));
+    };
+    if constexpr (IPT > 0) {
+#pragma unroll
+        for (int i = 0; i < IPT; ++i)
+            if (i * NT + (int)threadIdx.x < m) count(kr[i]);
+    } else {
+        for (int p = threadIdx.x; p < m; p += NT) count(keys[p]);
+    }
+    __syncthreads();
+    // exclusive scan over the bins in order: word w holds bins 2w (low
+    // half) and 2w + 1 (high half); each warp scans its WPW words
+    int carry = 0;
+    for (int r = 0; r < WPW / 32; ++r) {
+        const int w = warp * WPW + r * 32 + lane;
+        const uint32_t h = hist[w];
+        const int lo = (int)(h & 0xFFFFu), c = lo + (int)(h >> 16);
+        int incl = c;
+#pragma unroll
+        for (int of = 1; of < 32; of <<= 1) {
+            const int t = __shfl_up_sync(kFull, incl, of);
+            if (lane >= of) incl += t;
+        }
+        const int ex = carry + incl - c;
+        hist[w] = (uint32_t)ex | ((uint32_t)(ex + lo) << 16);
+        carry += __shfl_sync(kFull, incl, 31);
+    }
+    if (lane == 0) sm.scan[warp] = carry;
+    __syncthreads();
+    int wbase = 0;
+#pragma unroll
+    for (int w2 = 0; w2 < NW; ++w2) wbase += w2 < warp ? sm.scan[w2] : 0;
+    if (wbase)
+        for (int r = 0; r < WPW / 32; ++r) hist[warp * WPW + r * 32 + lane] += (uint32_t)wbase | ((uint32_t)wbase << 16);
+    __syncthreads();
+    auto place = [&](const uint64_t k) {
+        const uint32_t d = (uint32_t)(k >> shift) & (kBins - 1);
+        const uint32_t half = (d & 1u) << 4;
+        const uint32_t old = atomicAdd(&hist[d >> 1], 1u << half);
+        sm.k[(old >> half) & 0xFFFFu] = k;
+    };
+    if constexpr (IPT > 0) {
+#pragma unroll
+        for (int i = 0; i < IPT; ++i)
+            if (i * NT + (int)threadIdx.x < m) place(kr[i]);
+    } else {
+        for (int p = threadIdx.x; p < m; p += NT) place(keys[p]);
+    }
+    __syncthreads();
+    bool too_long = false;
+    for (int p = threadIdx.x; p < m; p += NT) {
+        const uint64_t k = sm.k[p];
+        const uint32_t d = (uint32_t)(k >> shift) & (kBins - 1);
+        const uint32_t e = (hist[d >> 1] >> ((d & 1u) << 4)) & 0xFFFFu;
+        const uint32_t s0 = d ? (hist[(d - 1) >> 1] >> (((d - 1) & 1u) << 4)) & 0xFFFFu : 0u;
+        if (e - s0 > (uint32_t)kMaxRankRun) {
+            too_long = true;
+            continue;
+        }
+        uint32_t rank = 0;
+        for (uint32_t q = s0; q < e; ++q) rank += key_before(sm.k[q], k, slot_gi) ? 1u : 0u;
+        out[s0 + rank] = (int32_t)(uint32_t)k;
+    }
+    return __syncthreads_or(too_long) != 0;
 }
 
 }  // namespace tilesort
