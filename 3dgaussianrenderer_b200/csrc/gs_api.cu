@@ -116,7 +116,8 @@ struct Counters {
     unsigned long long slots;                      // (view, Gaussian) slots taken by the frame kernel
     int64_t total;                                 // K
     int64_t sort_n;                                // min(K, key capacity)
-    unsigned int big_tiles;                        // tiles sorted ahead of the raster
+    unsigned int big_tiles;                        // tiles sorted ahead of the raster (to 4096 keys)
+    unsigned int huge_tiles;                       // those above 4096 keys
     unsigned int order_heads[2];                   // raster order: heavy tiles placed, others placed
     int err;
     int overflow;                                  // K > key capacity: the frame must be redone
@@ -616,7 +617,7 @@ int plan_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams,
     }
     if (sizeof(uint32_t) * tiles > ctx->tile_count.bytes) ctx->tile_count_dirty = true;
     if (ctx->ranges.ensure(sizeof(int32_t) * 2 * tiles) || ctx->tile_count.ensure(sizeof(uint32_t) * tiles) ||
-        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(sizeof(int32_t) * tiles) ||
+        ctx->cursor.ensure(sizeof(unsigned long long) * tiles) || ctx->big_list.ensure(sizeof(int32_t) * 2 * tiles) ||
         ctx->tile_order.ensure(sizeof(int32_t) * tiles))
         return fail(GS_ERR_OOM, "tile buffers");
     return GS_OK;
@@ -692,6 +693,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     ta.overflow = &dc->overflow;
     ta.big_list = ctx->big_list.as<int32_t>();
     ta.big_count = &dc->big_tiles;
+    ta.huge_count = &dc->huge_tiles;
     ta.fused_cap = fused_tile_capacity(cfg.tile_w, cfg.tile_h);
     launch_tile_scan(ta, st);
     launch_tile_order(ctx->ranges.as<int32_t>(), p.tiles_total, &dc->total, ctx->tile_order.as<int32_t>(),
@@ -727,6 +729,7 @@ int enqueue_bucket_frame(gs_ctx* ctx, const gs_scene* scene, const gs_render_cfg
     sa.slot_gi = ctx->offsets.as<int32_t>();
     sa.big_list = ctx->big_list.as<int32_t>();
     sa.big_count = &dc->big_tiles;
+    sa.huge_count = &dc->huge_tiles;
     sa.prefix_bits = cfg.sort_bits;
     if (p.n > 0) launch_tile_sort(sa, ctx->num_sms, st);
     GS_CUDA(record(ctx->ev[4], st, capturing));
@@ -950,11 +953,11 @@ int run_frame_bucket(gs_ctx* ctx, const gs_scene* scene, const gs_camera* cams, 
         stats->total_ms = ms_between(ctx->ev[0], ctx->ev[5]);
         stats->num_keys = ctx->h_counters->total;
         stats->num_tiles = p.tiles_total;
-        // frame kernel, bucket emit, big-tile sort; tile scan, tile order,
+        // frame kernel, bucket emit, the two big-tile sorts; tile scan, tile order,
         // raster (sorts the other tiles; one launch per view group when the
         // images stream to host memory group by group)
         const bool grouped = p.host_copy && p.host_copy->groups > 1 && cfg.termination == GS_TERM_TMIN;
-        stats->kernel_launches = (p.n > 0 ? 3 : 0) + 2 + (grouped ? p.host_copy->groups : 1);
+        stats->kernel_launches = (p.n > 0 ? 4 : 0) + 2 + (grouped ? p.host_copy->groups : 1);
         stats->graph_replay = replayed ? 1 : 0;
         stats->attempts = attempts;
     }

@@ -132,7 +132,10 @@ __global__ void __launch_bounds__(kThreads) tile_scan_kernel(TileScanArgs a)
     for (int j = 0; j < IPT; ++j) {
         const int64_t t = first + j;
         if (t < a.tiles) {
-            if (c[j] > (uint32_t)a.fused_cap) a.big_list[atomicAdd(a.big_count, 1u)] = (int32_t)t;
+            if (c[j] > (uint32_t)kTileSortSmemKeys)
+                a.big_list[a.tiles + atomicAdd(a.huge_count, 1u)] = (int32_t)t;
+            else if (c[j] > (uint32_t)a.fused_cap)
+                a.big_list[atomicAdd(a.big_count, 1u)] = (int32_t)t;
             a.cursor[t] = (unsigned long long)run;
             const int64_t lo = run < cap ? run : cap;
             const int64_t hi = run + c[j] < cap ? run + c[j] : cap;
@@ -354,7 +357,8 @@ void launch_emit_bucket(const BucketEmitArgs& a, int num_sms, cudaStream_t st)
 // (gs_tilesort.cuh).  The larger ones, listed by the tile scan, are sorted
 // here beforehand -- up to kTileSortSmemKeys keys by one counting pass in
 // shared memory and ranks inside its runs (tilesort::count_sort_tile; the
-// radix form of the raster CTA when a run is too long), else by stable LSD
+// radix form of the raster CTA when a run is too long), up to
+// kTileSortHugeKeys the same in one 1024-thread CTA, else by stable LSD
 // passes through global memory -- and their order is written to `vals` for
 // the rasteriser to read.  On the 64-view batch (57k such tiles, 92M keys)
 // the counting form takes 1.98 ms against 2.33 ms for the radix form.
@@ -529,12 +533,50 @@ __global__ void __launch_bounds__(kBigThreads, kBigBlocksPerSm) tile_sort_big_ke
     }
 }
 
+// The tiles above kTileSortSmemKeys keys, by persistent 1024-thread CTAs
+// (one per SM: 128 KB of keys and a 64 KB histogram of 2^15 bins in shared
+// memory), in the counting form over 15 depth bits.  A tile above
+// kTileSortHugeKeys keys, or with a run longer than kMaxRankRun, is handed
+// to tile_sort_big_kernel: appended to its list, which that kernel, launched
+// after this one on the same stream, reads when it starts.
+constexpr int kHugeThreads = 1024;
+constexpr int kHugeBits = 15;
+__global__ void __launch_bounds__(kHugeThreads, 1) tile_sort_huge_kernel(TileSortArgs a)
+{
+    constexpr int NW = kHugeThreads / 32;
+    extern __shared__ __align__(16) unsigned char smem[];
+    __shared__ int32_t s_scan[NW];
+    __shared__ uint64_t s_red[2 * NW];
+    Smem sm{};
+    sm.k = reinterpret_cast<uint64_t*>(smem);
+    sm.scan = s_scan;
+    sm.red = s_red;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(smem + kTileSortHugeKeys * 8);
+    const int nhuge = (int)*a.huge_count;
+    for (int j = blockIdx.x; j < nhuge; j += gridDim.x) {
+        const int64_t t = a.big_list[a.tiles + j];
+        const int64_t start = __ldg(&a.ranges[2 * t]);
+        const int m = __ldg(&a.ranges[2 * t + 1]) - (int)start;
+        bool handed = m > kTileSortHugeKeys;
+        if (!handed)
+            handed = tilesort::count_sort_tile<kHugeThreads, 0, kHugeBits>(a.keys + start, m, a.slot_gi, sm, hist,
+                                                                          a.vals + start);
+        if (handed && threadIdx.x == 0) a.big_list[atomicAdd(a.big_count, 1u)] = (int32_t)t;
+        __syncthreads();  // shared memory is reused by the next tile
+    }
+}
+
 void launch_tile_sort(const TileSortArgs& a, int num_sms, cudaStream_t st)
 {
     constexpr int big_smem = kTileSortSmemKeys * 12;
+    constexpr int huge_smem = kTileSortHugeKeys * 12;
     static PerDeviceOnce attr;
-    attr.run([] { cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big_smem); });
+    attr.run([] {
+        cudaFuncSetAttribute(tile_sort_big_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, big_smem);
+        cudaFuncSetAttribute(tile_sort_huge_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, huge_smem);
+    });
     if (a.tiles <= 0) return;
+    tile_sort_huge_kernel<<<(unsigned)num_sms, kHugeThreads, huge_smem, st>>>(a);
     tile_sort_big_kernel<<<(unsigned)(kBigBlocksPerSm * num_sms), kBigThreads, big_smem, st>>>(a);
 }
 

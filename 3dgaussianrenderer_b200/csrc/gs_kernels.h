@@ -158,8 +158,10 @@ struct TileScanArgs {
     int64_t capacity;
     int64_t* sort_n;                 // min(K, capacity)
     int* overflow;                   // K > capacity
-    int32_t* big_list;               // out: tiles with more than fused_cap keys
+    int32_t* big_list;               // out: [0, tiles) tiles with more than fused_cap keys, up to
+                                     // kTileSortSmemKeys; [tiles, 2 tiles) the larger ones
     unsigned int* big_count;
+    unsigned int* huge_count;
     int32_t fused_cap;
 };
 
@@ -174,11 +176,17 @@ struct TileSortArgs {
     int32_t* vals;                   // out: slots in blend order
     int32_t* vals_alt;
     const int32_t* slot_gi;
-    const int32_t* big_list;         // tiles above the fused capacity (from the tile scan)
-    const unsigned int* big_count;
+    int32_t* big_list;               // tiles above the fused capacity (from the tile scan; the
+                                     // tiles above kTileSortSmemKeys from index `tiles` on)
+    unsigned int* big_count;
+    const unsigned int* huge_count;
     int32_t prefix_bits;             // depth bits the radix passes sort (8..32; 0 = 16)
 };
 constexpr int kTileSortSmemKeys = 4096;
+// Tiles of up to this many keys are sorted in the shared memory of one
+// 1024-thread CTA (tile_sort_huge_kernel); larger ones by passes through
+// global memory.
+constexpr int kTileSortHugeKeys = 16384;
 // Keys a tile may have to be sorted inside its raster CTA (TW * TH / 2
 // threads, 8 keys each); larger tiles are sorted ahead of the raster.
 constexpr int kFusedIpt = 8;

@@ -314,13 +314,13 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
 }
 
 // Counting-sort form of sort_tile for the stand-alone sort of the larger
-// tiles (m <= kTileSortSmemKeys keys, NT threads), writing the tile's slots
-// in (depth, index) order to `out`.  One pass places every key in shared
-// memory by the top kCountBits varying depth bits: a histogram of 16-bit
-// counters packed two to a word (`hist`, 2^(kCountBits - 1) words; counts
-// and offsets stay below 2^16), its exclusive scan, then each key takes the
-// next position of its bin with a shared-memory atomic, so inside a bin the
-// keys land in no particular order.  After the placement the histogram
+// tiles (m keys, as many as sm.k holds; NT threads), writing the tile's
+// slots in (depth, index) order to `out`.  One pass places every key in shared
+// memory by the top BITS varying depth bits: a histogram of 16-bit
+// counters packed two to a word (`hist`, 2^(BITS - 1) words; counts and
+// offsets stay below 2^16, so m < 2^16), its exclusive scan, then each key
+// takes the next position of its bin with a shared-memory atomic, so inside
+// a bin the keys land in no particular order.  After the placement the histogram
 // holds every bin's end, and each key's bin is the run [end(d - 1), end(d))
 // of the keys with its prefix: the key's rank among them in (depth, index)
 // order, counted by the key's own thread, is its offset in the run.  That
@@ -330,18 +330,18 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
 // IPT > 0: m <= NT * IPT, each thread holds its IPT keys in registers
 // across the passes; IPT = 0: every pass reads the keys from global memory
 // (the larger tiles).
-// Returns true -- nothing written -- when some run is longer than
-// kMaxRankRun; the caller then sorts the tile another way.  Every thread of
+// Returns true when some run is longer than kMaxRankRun (`out` then holds
+// only part of the order); the caller then sorts the tile another way.  Every thread of
 // the CTA must call it; it ends with a barrier.
 constexpr int kCountBits = 13;
 constexpr int kMaxRankRun = 64;
 
-template <int NT, int IPT>
+template <int NT, int IPT, int BITS = kCountBits>
 __device__ bool count_sort_tile(const uint64_t* __restrict__ keys, const int m, const int32_t* __restrict__ slot_gi,
                                 const Smem& sm, uint32_t* hist, int32_t* __restrict__ out)
 {
     constexpr int NW = NT / 32;
-    constexpr int kBins = 1 << kCountBits;
+    constexpr int kBins = 1 << BITS;
     constexpr int kWords = kBins / 2;
     constexpr int WPW = kWords / NW;  // histogram words scanned by each warp
     static_assert(WPW % 32 == 0, "histogram words per warp");
@@ -367,7 +367,7 @@ __device__ bool count_sort_tile(const uint64_t* __restrict__ keys, const int m, 
     }
     for (int w = threadIdx.x; w < kWords; w += NT) hist[w] = 0u;
     int shift;
-    prefix_window(varying_bits<NT>(o, n, sm.red) & 0xFFFFFFFF00000000ull, kCountBits, &shift);
+    prefix_window(varying_bits<NT>(o, n, sm.red) & 0xFFFFFFFF00000000ull, BITS, &shift);
     // (varying_bits ends with a barrier: the cleared histogram is visible)
     auto count = [&](const uint64_t k) {
         const uint32_t d = (uint32_t)(k >> shift) & (kBins - 1);
