@@ -169,6 +169,38 @@ def test_bench_views_raster_vs_oracle_raster(gs, O, bench3):
         assert p >= PSNR_MIN
 
 
+def test_bench_views_tuned_knobs_vs_oracle_raster(gs, O, bench3):
+    """The knobs the autotuner picks for the benchmark (64-entry raster
+    chunks, 32 views per block) against the oracle's raster of the same
+    lists: the chunk size moves only where a warp stops after its pixels
+    fell below t_min, the view grouping nothing."""
+    d = bench3
+    n = d["n"]
+    rc = gs.RenderConfig(raster_chunk=64, views_per_block=32)
+    ctx = gs.Context(0)
+    scene = gs.Scene(ctx, d["sc"]["pos4"], d["sc"]["sr4"], d["sh"], 3)
+    total = sum(c.GetWidth() * c.GetHeight() * 4 for c in d["cams"])
+    host = np.zeros(total, np.uint8)
+    gs.render_batch_host(ctx, scene, d["cams"], rc, host)
+    scene.close()
+    ctx.close()
+    off = 0
+    for v, cam in enumerate(d["cams"]):
+        W, H = cam.GetWidth(), cam.GetHeight()
+        img = host[off:off + W * H * 4].reshape(H, W, 4)
+        off += W * H * 4
+        s = slice(v * n, (v + 1) * n)
+        k, val = O.build(d["xy"][s], d["ell"][s], d["z"][s], cam, d["rc"])
+        T = gs.num_tiles(W, H, d["rc"])
+        sk, sv = O.sort(k, val, gs.key_bits(T))
+        oimg = O.raster(cam, d["rc"], O.ranges(sk, T), sv, d["xy"][s], d["con"][s], d["col"][s])
+        diff = np.abs(img.astype(int) - oimg.astype(int))
+        p = psnr(img, oimg)
+        print(f"view {v} (64-entry chunks): max diff {diff.max()}, psnr {p:.2f} dB")
+        assert diff.max() <= IMG_TOL
+        assert p >= PSNR_MIN
+
+
 def test_bench_views_end_to_end_vs_oracle(gs, O, bench3):
     """The GPU's images against the oracle's whole frame (its own SH,
     projection, build, sort and raster)."""
