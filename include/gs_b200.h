@@ -80,8 +80,10 @@ typedef struct gs_render_cfg {
                               step, 32 or 64 (0 = 32) */
     int32_t raster_persistent; /* GS_TERM_TMIN raster: 1 = persistent CTAs pulling tiles (heavy first) from an
                               atomic queue; 0 (default) = one CTA per tile */
-    int32_t sort_bits;     /* per-tile depth sort of GS_ORDER_BUCKETS frames: the top varying depth bits sorted by
-                              radix passes, 8..32 (0 = 16); the rest is ordered by insertion within runs */
+    int32_t sort_bits;     /* per-tile depth sort of GS_ORDER_BUCKETS frames inside the raster CTA: the top
+                              varying depth bits sorted by radix passes, 8..32 (0 = 16); the rest is ordered by
+                              insertion within runs.  The larger tiles, sorted ahead of the raster, use one
+                              counting pass over 13 or 15 bits and fall back on this form for long runs */
 } gs_render_cfg;
 
 /* Tile-list ordering of the whole-frame entry points.  Both give the order of
