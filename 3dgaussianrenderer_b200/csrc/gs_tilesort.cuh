@@ -315,24 +315,25 @@ __device__ void sort_tile(const uint64_t* __restrict__ keys, const int m, const 
 
 // Counting-sort form of sort_tile for the stand-alone sort of the larger
 // tiles (m keys, as many as sm.k holds; NT threads), writing the tile's
-// slots in (depth, index) order to `out`.  One pass places every key in shared
-// memory by the top BITS varying depth bits: a histogram of 16-bit
+// slots in (depth, index) order to `out`.  One pass places every key in
+// shared memory by the top BITS varying depth bits: a histogram of 16-bit
 // counters packed two to a word (`hist`, 2^(BITS - 1) words; counts and
 // offsets stay below 2^16, so m < 2^16), its exclusive scan, then each key
-// takes the next position of its bin with a shared-memory atomic, so inside
-// a bin the keys land in no particular order.  After the placement the histogram
-// holds every bin's end, and each key's bin is the run [end(d - 1), end(d))
-// of the keys with its prefix: the key's rank among them in (depth, index)
-// order, counted by the key's own thread, is its offset in the run.  That
-// is the whole order (keys of different bins are ordered by the bin), so
-// the pass need not be stable, and a run of L keys costs L comparisons per
-// key, in parallel.  On the benchmark's views no run is longer than 25 keys.
+// takes the next position of its bin with a shared-memory atomic, so
+// inside a bin the keys land in no particular order.  After the placement
+// the histogram holds every bin's end, and each key's bin is the run
+// [end(d - 1), end(d)) of the keys with its prefix: the key's rank among
+// them in (depth, index) order, counted by the key's own thread, is its
+// offset in the run.  That is the whole order (keys of different bins are
+// ordered by the bin), so the pass need not be stable, and a run of L keys
+// costs L comparisons per key, in parallel.  The callers keep about two
+// bins per key (13 bits for up to 4096 keys, 15 for up to 16384); at 13
+// bits no run on the benchmark's views is longer than 25 keys.
 // IPT > 0: m <= NT * IPT, each thread holds its IPT keys in registers
-// across the passes; IPT = 0: every pass reads the keys from global memory
-// (the larger tiles).
+// across the passes; IPT = 0: every pass reads the keys from global memory.
 // Returns true when some run is longer than kMaxRankRun (`out` then holds
-// only part of the order); the caller then sorts the tile another way.  Every thread of
-// the CTA must call it; it ends with a barrier.
+// only part of the order); the caller then sorts the tile another way.
+// Every thread of the CTA must call it; it ends with a barrier.
 constexpr int kCountBits = 13;
 constexpr int kMaxRankRun = 64;
 
