@@ -106,25 +106,68 @@ __device__ __forceinline__ unsigned lane_range_mask(const int lo, const int hi)
 // arithmetic.  Keeping the IEEE code out of the first walk keeps it free of
 // register spills.
 __device__ __forceinline__ void add_hits(const unsigned bal, const WarpCands& w, const int base, const int cand,
-                                         int& hits, uint32_t& mask)
+                                         const int c0, int& hits, uint32_t& mask)
 {
     const unsigned bits = bal & lane_range_mask(max(w.excl - base, 0), min(w.incl - base, 32));
     if (bits) {
         hits += __popc(bits);
-        // lane l of this chunk is candidate base + l - excl of its owner
-        if (cand <= 32) mask |= (w.excl >= base) ? (bits >> (w.excl - base)) : (bits << (base - w.excl));
+        if (cand <= 32) {
+            // lane l of this chunk is walk index base + l - excl of its
+            // owner; the walk skips the owner's centre candidate c0
+            uint32_t mk = (w.excl >= base) ? (bits >> (w.excl - base)) : (bits << (base - w.excl));
+            if (c0 >= 0) {
+                const uint32_t low = (1u << c0) - 1u;
+                mk = (mk & low) | ((mk & ~low) << 1);
+            }
+            mask |= mk;
+        }
     }
 }
+
+// The candidate index in the owner's rectangle of walk index k: the walk
+// leaves out the owner's centre candidate oc0 (counted before the walk).
+__device__ __forceinline__ int walk_candidate(const int k, const int oc0) { return (oc0 >= 0 && k >= oc0) ? k + 1 : k; }
 
 __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const int cand, const ViewParams& v,
                                                uint32_t& mask, uint32_t* tile_count = nullptr,
                                                const bool aggregate = false)
 {
     const int lane = threadIdx.x & 31;
-    const WarpCands w = warp_scan_cands(cand);
-    int hits = 0;
-    mask = 0u;
+    // The tile holding the centre is a hit (the centre test decides it):
+    // each lane counts its own before the walk, which then leaves it out --
+    // half of the candidates on the benchmark's views.  The tile is found
+    // with the tile rectangle's own arithmetic and confirmed with the
+    // centre test's; a centre on a tile border falls through to the walk.
+    int c0 = -1, tile0 = 0;
+    if (cand > 0) {
+        const int gx = (int)floorf((e.cx + 1.0f) * 0.5f * v.tiles_xf);
+        const int gy = (int)floorf((e.cy + 1.0f) * 0.5f * v.tiles_yf);
+        const int lx = gx - r.x, ly = gy - r.y;
+        if (lx >= 0 && lx < r.z && ly >= 0 && ly < r.w && gx >= 0 && gx < v.tiles_x && gy >= 0 && gy < v.tiles_y) {
+            float x0, y0, x1, y1;
+            tile_clip_rect(v, gx, gy, x0, y0, x1, y1);
+            if (e.cx > x0 && e.cx < x1 && e.cy > y0 && e.cy < y1) {
+                c0 = ly * r.z + lx;
+                tile0 = gy * v.tiles_x + gx;
+            }
+        }
+    }
+    const bool pre = c0 >= 0;
+    const WarpCands w = warp_scan_cands(cand - (pre ? 1 : 0));
+    int hits = pre ? 1 : 0;
+    mask = (pre && cand <= 32) ? (1u << c0) : 0u;
     bool undecided = false;
+    {
+        const unsigned bal = __ballot_sync(kFull, pre);
+        if (tile_count && pre) {
+            if (aggregate) {
+                const unsigned grp = __match_any_sync(bal, tile0);
+                if (lane == __ffs(grp) - 1) atomicAdd(&tile_count[v.tile_offset + tile0], (unsigned)__popc(grp));
+            } else {
+                atomicAdd(&tile_count[v.tile_offset + tile0], 1u);
+            }
+        }
+    }
     auto owner_ell = [&](const int o, Ell& oe, int4& orr) {
         oe.cx = __shfl_sync(kFull, e.cx, o);
         oe.cy = __shfl_sync(kFull, e.cy, o);
@@ -144,9 +187,10 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
         int4 orr;
         owner_ell(o, oe, orr);
         const int oexcl = __shfl_sync(kFull, w.excl, o);
+        const int oc0 = __shfl_sync(kFull, c0, o);
         int st = 0;
         int tile = 0;
-        if (c < w.total) st = candidate_state(oe, orr, c - oexcl, v, tile);
+        if (c < w.total) st = candidate_state(oe, orr, walk_candidate(c - oexcl, oc0), v, tile);
         undecided |= st < 0;
         const bool hit = st > 0;
         const unsigned bal = __ballot_sync(kFull, hit);
@@ -158,7 +202,7 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
                 atomicAdd(&tile_count[v.tile_offset + tile], 1u);
             }
         }
-        add_hits(bal, w, base, cand, hits, mask);
+        add_hits(bal, w, base, cand, c0, hits, mask);
     }
     if (__any_sync(kFull, undecided)) {
         // rare: the candidates too close to call, in IEEE arithmetic
@@ -169,13 +213,15 @@ __device__ __forceinline__ int warp_count_hits(const Ell& e, const int4 r, const
             int4 orr;
             owner_ell(o, oe, orr);
             const int oexcl = __shfl_sync(kFull, w.excl, o);
+            const int oc0 = __shfl_sync(kFull, c0, o);
             int tile = 0;
             bool hit = false;
-            if (c < w.total && candidate_state(oe, orr, c - oexcl, v, tile) < 0) hit = candidate_hit_ieee(oe, tile, v);
+            const int oc = walk_candidate(c - oexcl, oc0);
+            if (c < w.total && candidate_state(oe, orr, oc, v, tile) < 0) hit = candidate_hit_ieee(oe, tile, v);
             const unsigned bal = __ballot_sync(kFull, hit);
             if (!bal) continue;
             if (tile_count && hit) atomicAdd(&tile_count[v.tile_offset + tile], 1u);
-            add_hits(bal, w, base, cand, hits, mask);
+            add_hits(bal, w, base, cand, c0, hits, mask);
         }
     }
     return hits;
