@@ -385,8 +385,9 @@ __device__ __forceinline__ bool hits_unit_circle(const float v0x, const float v0
     return len2(prx, pry) < 1.0f;
 }
 
-// The five tests evaluated with the hardware reciprocal, each result kept
-// as the value compared with 1.  Returns 1 (overlap) or 0 (none) when every
+// The reference's tests evaluated with the hardware reciprocal, each result
+// kept as the value compared with 1 (the rectangle centre and the nearer
+// edge of each parallel pair; see below).  Returns 1 (overlap) or 0 (none) when every
 // value lies clearly on one side of 1, -1 otherwise.  "Clearly" is a margin
 // from an error bound.  Both evaluations start from the same corners, centre,
 // axis and extents.  Let R be D / min(ex, ey), where D bounds the image-space
@@ -476,20 +477,25 @@ __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const fl
     };
     // rect centre in the ellipse
     if (test(len2(ax + 0.5f * (ux + vx), ay + 0.5f * (uy + vy)))) return 1;
-    // the four edges: the point of segment p + t d (t in [0, 1]) nearest
-    // the origin
+    // the edges: the point of segment p + t d (t in [0, 1]) nearest the
+    // origin.  Of two parallel edges only the nearer line's is needed: both
+    // span the same range along their direction, so the farther one's
+    // squared length is the nearer one's plus the difference of the squared
+    // line distances.  Where the nearer edge's value lies clearly above 1,
+    // the farther edge's does too; where the two are nearly equally far,
+    // either gives nearly the same value.
     const float iu = rcp_approx(len2(ux, uy)), iv = rcp_approx(len2(vx, vy));
     auto edge = [](const float px, const float py, const float dx, const float dy, const float inv) {
         const float t = __saturatef(-(px * dx + py * dy) * inv);
         return len2(px + t * dx, py + t * dy);
     };
-    const float bx = ax + ux, by = ay + uy;  // (x1, y0)
-    const float cx = bx + vx, cy = by + vy;  // (x1, y1)
-    const float qx = ax + vx, qy = ay + vy;  // (x0, y1)
-    if (test(edge(ax, ay, ux, uy, iu))) return 1;
-    if (test(edge(bx, by, vx, vy, iv))) return 1;
-    if (test(edge(cx, cy, -ux, -uy, iu))) return 1;
-    if (test(edge(qx, qy, -vx, -vy, iv))) return 1;
+    // u edges through a (x0, y0) and a + v (x0, y1); v edges through a and
+    // a + u (x1, y0): compare the lines' distances by cross products
+    const float su = ax * uy - ay * ux, kuv = vx * uy - vy * ux, sv = ax * vy - ay * vx;
+    const bool u_at_a = fabsf(su) <= fabsf(su + kuv);
+    const bool v_at_a = fabsf(sv) <= fabsf(sv - kuv);
+    if (test(edge(u_at_a ? ax : ax + vx, u_at_a ? ay : ay + vy, ux, uy, iu))) return 1;
+    if (test(edge(v_at_a ? ax : ax + ux, v_at_a ? ay : ay + uy, vx, vy, iv))) return 1;
     return unclear ? -1 : 0;
 }
 

@@ -4,8 +4,9 @@ restated in single precision with numpy, against the oracle's IEEE test
 (core/gaussian_render.cu:250-272 via oracle/gs_oracle.c).
 
 The cheap evaluation computes the tile's corners in ellipse coordinates as
-a parallelogram with hardware reciprocals; it may only decide a candidate
-when every compared value lies more than 256 u R + 2^-15 from 1 (u = 2^-24,
+a parallelogram with hardware reciprocals and compares the rectangle centre
+and, of each pair of parallel edges, the nearer one; it may only decide a
+candidate when every compared value lies more than 256 u R + 2^-15 from 1 (u = 2^-24,
 R = image-space corner offset / smallest extent).  Here every decided
 candidate must agree with the oracle, with the reciprocals perturbed by one
 ulp either way, and the measured difference of the compared values must stay
@@ -77,9 +78,35 @@ def _cheap(e, r, jitter):
     return np.stack(vals), margin, R
 
 
+def _cheap_nearer(e, r, jitter):
+    """The values the kernel compares: the rectangle centre and, of each
+    pair of parallel edges, the one on the line nearer the origin (chosen by
+    cross products, as in the kernel)."""
+    cx, cy, cs, sn, ex, ey = e
+    x0, y0, x1, y1 = r
+    vals5, margin, _ = _cheap(e, r, jitter)
+    with np.errstate(all="ignore"):
+        iex, iey = _rcp(ex, jitter), _rcp(ey, -jitter)
+        dx0, dy0 = (x0 - cx).astype(f), (y0 - cy).astype(f)
+        ax = ((dx0 * cs + dy0 * sn) * iex).astype(f)
+        ay = ((dy0 * cs - dx0 * sn) * iey).astype(f)
+        w, h = (x1 - x0).astype(f), (y1 - y0).astype(f)
+        ux, uy = ((w * cs) * iex).astype(f), (-(w * sn) * iey).astype(f)
+        vx, vy = ((h * sn) * iex).astype(f), ((h * cs) * iey).astype(f)
+        su = (ax * uy - ay * ux).astype(f)
+        kuv = (vx * uy - vy * ux).astype(f)
+        sv = (ax * vy - ay * vx).astype(f)
+        u_at_a = np.abs(su) <= np.abs((su + kuv).astype(f))
+        v_at_a = np.abs(sv) <= np.abs((sv - kuv).astype(f))
+    # vals5: centre, edge (a, u), edge (a + u, v), edge (a + u + v, -u), edge (a + v, -v)
+    eu = np.where(u_at_a, vals5[1], vals5[3])
+    ev = np.where(v_at_a, vals5[4], vals5[2])
+    return np.stack([vals5[0], eu, ev]), margin
+
+
 def _decide(e, r, jitter):
     """1 / 0 / -1 as ellipse_rect_overlap_clear, after the caller's centre test."""
-    vals, margin, _ = _cheap(e, r, jitter)
+    vals, margin = _cheap_nearer(e, r, jitter)
     zero = (e[4] == 0) | (e[5] == 0)
     with np.errstate(invalid="ignore"):
         hit = np.any(vals < 1 - margin, axis=0)
