@@ -356,20 +356,13 @@ struct Ell {
     float cx, cy, cs, sn, ex, ey;
 };
 
-// FAST (the approximate pre-check of ellipse_rect_overlap_clear): the
-// divisions by the extents become multiplications by hardware reciprocals.
-template <bool FAST>
-__device__ __forceinline__ void to_ellipse(const Ell& e, const float px, const float py, float& ox, float& oy,
-                                           const float iex, const float iey)
+// A point in the ellipse's frame, in units of its extents
+// (convertToEllipseCoordinates, gaussian_render.cu:234-240).
+__device__ __forceinline__ void to_ellipse(const Ell& e, const float px, const float py, float& ox, float& oy)
 {
     const float dx = px - e.cx, dy = py - e.cy;
-    if constexpr (FAST) {
-        ox = (dx * e.cs + dy * e.sn) * iex;
-        oy = (dy * e.cs - dx * e.sn) * iey;
-    } else {
-        ox = (dx * e.cs + dy * e.sn) / e.ex;
-        oy = (dy * e.cs - dx * e.sn) / e.ey;
-    }
+    ox = (dx * e.cs + dy * e.sn) / e.ex;
+    oy = (dy * e.cs - dx * e.sn) / e.ey;
 }
 
 __device__ __forceinline__ float len2(const float x, const float y) { return x * x + y * y; }
@@ -411,18 +404,17 @@ __device__ __forceinline__ int ellipse_rect_overlap_clear(const Ell& e, const fl
 static __device__ __noinline__ bool ellipse_rect_overlap_ieee(const Ell e, const float x0, const float y0, const float x1,
                                                        const float y1)
 {
-    const float iex = 0.0f, iey = 0.0f;
     // Rect::getCenter = min + (max - min) * 0.5
     const float rcx = x0 + (x1 - x0) * 0.5f;
     const float rcy = y0 + (y1 - y0) * 0.5f;
     float ux, uy;
-    to_ellipse<false>(e, rcx, rcy, ux, uy, iex, iey);
+    to_ellipse(e, rcx, rcy, ux, uy);
     bool ov = len2(ux, uy) < 1.0f;
     float p0x, p0y, p1x, p1y, p2x, p2y, p3x, p3y;
-    to_ellipse<false>(e, x0, y0, p0x, p0y, iex, iey);
-    to_ellipse<false>(e, x1, y0, p1x, p1y, iex, iey);
-    to_ellipse<false>(e, x1, y1, p2x, p2y, iex, iey);
-    to_ellipse<false>(e, x0, y1, p3x, p3y, iex, iey);
+    to_ellipse(e, x0, y0, p0x, p0y);
+    to_ellipse(e, x1, y0, p1x, p1y);
+    to_ellipse(e, x1, y1, p2x, p2y);
+    to_ellipse(e, x0, y1, p3x, p3y);
     ov |= hits_unit_circle(p0x, p0y, p1x, p1y);
     ov |= hits_unit_circle(p1x, p1y, p2x, p2y);
     ov |= hits_unit_circle(p2x, p2y, p3x, p3y);
